@@ -1,0 +1,193 @@
+/*
+ * hm.h -- C ABI of the B200 hierarchical-matrix engine (libhmb200.so).
+ *
+ * The entry points replace the reference's pipeline functions one for one
+ * (citations are file:line in the reference project):
+ *
+ *   hm_generate_dataset     generateDataset              src/generateDataset.cu:15-19
+ *   hm_kdtree_build         allocateKDTree+constructKDTree src/kDTree.cu:6-31,
+ *                                                         src/kDTreeConstruction.cu:14-231
+ *   hm_kdtree_copy_out      KDTree / KDTreeBoundingBoxes   src/kDTree.cuh:8-14,
+ *                           (perm, offsets, boxes)         src/boundingBoxes.h:8-23
+ *   hm_structure_build      constructHMatrixStructure      src/HMatrixStructure.cu:133-160
+ *   hm_structure_tiles      HMatrixStructure.tileIndices   src/HMatrixStructure.cuh:8-13
+ *   hm_tlr_build            createColumnMajorLRMatrix      src/constructTLRMatrix.cu:13-151
+ *   hm_hmatrix_build        allocateHMatrix +              src/HMatrix.cu:57-103,
+ *                           generateHMatrixFromStruct      src/constructHMatrixFromStruct.cu:13-103
+ *   hm_hmatvec              HMatrixVecMult                 src/HMatrixVectorMultiplication.cu:10-27
+ *   hm_*_free               freeKDTree / freeMatrix /      src/kDTree.cu:33-36, src/TLRMatrix.cu:5,
+ *                           freeHMatrix / freeHMatrixStructure src/HMatrix.cu:105-110,
+ *                                                         src/HMatrixStructure.cu:162-168
+ *
+ * Conventions.  Every function returns an hm_status and never exits the
+ * process; hm_last_error() gives a message for the last failure on the calling
+ * thread.  Points are caller-owned device buffers in the reference's SoA
+ * layout p[dim*n + i].  Vectors are caller-owned device buffers, column-major
+ * n x nrhs.  `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ * stream).  Objects are opaque handles owned by the library; one handle may be
+ * used by one host thread at a time.
+ */
+#ifndef HM_H
+#define HM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HM_API __attribute__((visibility("default")))
+#else
+#define HM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  HM_OK = 0,
+  HM_ERR_INVALID = 1,       /* bad argument (null pointer, size, enum) */
+  HM_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+  HM_ERR_NOMEM = 3,         /* device or host allocation failed */
+  HM_ERR_UNSUPPORTED = 4,   /* valid request outside what this build supports */
+  HM_ERR_TIMEOUT = 5        /* a bounded device-side wait gave up */
+} hm_status;
+
+typedef enum { HM_ADMISS_WEAK = 0, HM_ADMISS_BOX_CENTER = 1 } hm_admissibility;
+
+typedef enum {
+  HM_KERNEL_EXP = 0,       /* exp(-r/l)                       src/TLRMatrixHelpers.cu:44-58 */
+  HM_KERNEL_MATERN32 = 1,  /* (1 + sqrt3 r/l) exp(-sqrt3 r/l) */
+  HM_KERNEL_GAUSS = 2      /* exp(-r^2 / (2 l^2))             */
+} hm_kernel;
+
+typedef enum {
+  HM_PREC_FP32 = 0,        /* FP32 factors, FP32 arithmetic */
+  HM_PREC_MIXED = 1        /* BF16 factors with a BF16 low part where the tolerance needs it */
+} hm_precision;
+
+typedef struct hm_kdtree_s* hm_kdtree;
+typedef struct hm_structure_s* hm_structure;
+typedef struct hm_hmatrix_s* hm_hmatrix;
+
+/* Message describing the last failure on this thread ("" if none). */
+HM_API const char* hm_last_error(void);
+
+/* Library version string. */
+HM_API const char* hm_version(void);
+
+/* --- points ------------------------------------------------------------- */
+
+/* generateDataset (src/generateDataset.cu:15-19): d_points[i] for i < n*d is
+ * curand_uniform of a XORWOW state initialised with (seed, subsequence i, 0).
+ * seed = 1234 reproduces the reference bit for bit. */
+HM_API hm_status hm_generate_dataset(int n, int d, unsigned long long seed, double* d_points,
+                              void* stream);
+
+/* --- KD tree ------------------------------------------------------------ */
+
+/* allocateKDTree + constructKDTree, FULL_TREE division
+ * (src/kDTree.cu:6-31, src/kDTreeConstruction.cu:14-231).  The permutation,
+ * leaf offsets and per-level boxes equal the reference's bit for bit.
+ * d_points is read during the call only.  bucket >= 1; n >= 1; 1 <= d <= 16. */
+HM_API hm_status hm_kdtree_build(const double* d_points, int n, int d, int bucket, void* stream,
+                          hm_kdtree* out);
+
+/* depth = number of levels below the root; leaves = 2^depth. */
+HM_API hm_status hm_kdtree_info(hm_kdtree t, int* n, int* d, int* bucket, int* depth);
+
+/* Host copies.  Any pointer may be NULL.  perm: n ints (tree position ->
+ * original index, segmentIndices); offsets: 2^depth+1 ints (segmentOffsets);
+ * bmin/bmax: levels 0..depth, level l at [(2^l - 1)*d], node-major
+ * [node*d + dim] (levels 0..depth-1 are the reference's
+ * KDTreeBoundingBoxes); split_dim: levels 0..depth-1, level l at [2^l - 1]. */
+HM_API hm_status hm_kdtree_copy_out(hm_kdtree t, int* perm, int* offsets, double* bmin, double* bmax,
+                             int* split_dim);
+
+/* Device pointers owned by the tree (valid until hm_kdtree_free). */
+HM_API const int* hm_kdtree_device_perm(hm_kdtree t);
+HM_API const int* hm_kdtree_device_offsets(hm_kdtree t);
+
+HM_API void hm_kdtree_free(hm_kdtree t);
+
+/* --- block structure ----------------------------------------------------- */
+
+/* constructHMatrixStructure (src/HMatrixStructure.cu:133-160): per level
+ * l = 1..depth the list of blocks recorded at that level, as Morton indices
+ * z = interleave(column cluster) | interleave(row cluster) << 1, in the
+ * reference's order.  eta is the box-center parameter (the reference fixes
+ * 1.0, src/HMatrixStructure.cu:7). */
+HM_API hm_status hm_structure_build(hm_kdtree t, int admissibility, double eta, void* stream,
+                             hm_structure* out);
+
+/* num_levels = depth + 1 as in the reference; counts[l-1] for l = 1..depth
+ * (counts needs num_levels - 1 entries; may be NULL). */
+HM_API hm_status hm_structure_info(hm_structure s, int* num_levels, int* counts);
+
+/* Host copy of the Morton list of level l (1 <= l <= depth). */
+HM_API hm_status hm_structure_tiles(hm_structure s, int level, int* tiles);
+
+/* Row-major (CSR) and jagged-diagonal (JDS) layouts of level l, built on the
+ * device (the reference's JDS.cuh declares HMatrixLevelJDS, src/JDS.cuh:7-17,
+ * but never fills it).  Any pointer may be NULL.  row_ptr: 2^l + 1; csr_blk:
+ * counts[l-1] indices into the level's Morton list, grouped by row cluster,
+ * increasing column within a row; jds_rows: 2^l row clusters by decreasing
+ * block count; jds_ptr: max_row_blocks + 1 diagonal starts; jds_blk:
+ * counts[l-1] entries, jds_blk[jds_ptr[j] + r] = j-th block of row jds_rows[r]. */
+HM_API hm_status hm_structure_jds(hm_structure s, int level, int* row_ptr, int* csr_blk,
+                                  int* jds_rows, int* jds_ptr, int* jds_blk, int* max_row_blocks);
+
+HM_API void hm_structure_free(hm_structure s);
+
+/* --- H-matrix ------------------------------------------------------------ */
+
+typedef struct {
+  int kernel;          /* hm_kernel */
+  double ell;          /* length scale */
+  double nugget;       /* added to the diagonal */
+  double tol;          /* per-block relative Frobenius tolerance */
+  int max_rank;        /* rank cap for admissible blocks above the leaf level */
+  int leaf_max_rank;   /* rank cap for leaf-level blocks (reference: bucket/2); 0 = bucket/2 */
+  int sample_block;    /* ARA sample block (reference: 16) */
+  int precision;       /* hm_precision */
+  int derivative;      /* 0: K, 1: dK/dl */
+  unsigned long long seed;  /* seed of the Gaussian test matrices */
+} hm_build_opts;
+
+/* Fills opts with the reference's settings: exp kernel, l = 0.2 if d == 3
+ * else 0.1 (src/TLRMatrixHelpers.cu:40-42), tol 1e-5, sample block 16. */
+HM_API void hm_build_opts_default(int d, hm_build_opts* opts);
+
+/* allocateHMatrix + generateHMatrixFromStruct: compresses every block of the
+ * structure by adaptive randomized approximation on kernel entries generated
+ * from the points, leaf diagonal blocks dense.  d_points: the points the tree
+ * was built from. */
+HM_API hm_status hm_hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points,
+                           const hm_build_opts* opts, void* stream, hm_hmatrix* out);
+
+typedef struct {
+  long long num_lowrank;     /* low-rank blocks (each stored pair counted twice) */
+  long long num_dense;       /* dense blocks, diagonal leaves included */
+  long long rank_sum;        /* sum of ranks over low-rank blocks */
+  int max_rank_seen;
+  long long factor_bytes;    /* bytes of stored factors */
+  long long dense_bytes;     /* bytes of stored dense blocks */
+  long long matvec_bytes_per_rhs; /* unused, 0 */
+  double build_seconds;      /* device time of hm_hmatrix_build */
+} hm_hmatrix_stats;
+
+HM_API hm_status hm_hmatrix_stats_get(hm_hmatrix h, hm_hmatrix_stats* st);
+
+/* Y = H X (trans = 0) or Y = H^T X (trans = 1).  X, Y: device, column-major
+ * n x nrhs with leading dimensions ldx, ldy >= n, FP32.  original_order = 0:
+ * X and Y are in tree order (the reference's convention); 1: in the points'
+ * original order (the permutation is applied inside).  No allocation and no
+ * host synchronisation: the call is stream-ordered. */
+HM_API hm_status hm_hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, int ldx, float* Y,
+                     int ldy, int original_order, void* stream);
+
+HM_API void hm_hmatrix_free(hm_hmatrix h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HM_H */

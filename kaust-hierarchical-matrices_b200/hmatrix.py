@@ -1,0 +1,226 @@
+"""Python host binding of libhmb200.so (ctypes over the C ABI in include/hm.h).
+
+Mirrors the reference's pipeline operators (reference file:line):
+
+    generate_dataset            generateDataset            src/generateDataset.cu:15-19
+    construct_kdtree            allocateKDTree +           src/kDTree.cu:6-31,
+                                constructKDTree            src/kDTreeConstruction.cu:14-231
+    construct_hmatrix_structure constructHMatrixStructure  src/HMatrixStructure.cu:133-160
+    build_hmatrix               allocateHMatrix +          src/HMatrix.cu:57-103,
+                                generateHMatrixFromStruct  src/constructHMatrixFromStruct.cu:13-103
+    HMatrix.matvec              HMatrixVecMult             src/HMatrixVectorMultiplication.cu:10-27
+
+Device memory comes from torch tensors (plumbing only); all computation runs in
+the CUDA kernels of libhmb200.so.  There is no fallback: if the library is
+missing the import-time loader raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhmb200.so")
+
+WEAK, BOX_CENTER = 0, 1
+K_EXP, K_MATERN32, K_GAUSS = 0, 1, 2
+PREC_FP32, PREC_MIXED = 0, 1
+
+
+class HMError(RuntimeError):
+    """A libhmb200 call returned a non-zero hm_status."""
+
+    def __init__(self, status, msg):
+        super().__init__("hm status %d: %s" % (status, msg))
+        self.status = status
+
+
+class BuildOpts(ctypes.Structure):
+    _fields_ = [
+        ("kernel", ctypes.c_int),
+        ("ell", ctypes.c_double),
+        ("nugget", ctypes.c_double),
+        ("tol", ctypes.c_double),
+        ("max_rank", ctypes.c_int),
+        ("leaf_max_rank", ctypes.c_int),
+        ("sample_block", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("derivative", ctypes.c_int),
+        ("seed", ctypes.c_ulonglong),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("num_lowrank", ctypes.c_longlong),
+        ("num_dense", ctypes.c_longlong),
+        ("rank_sum", ctypes.c_longlong),
+        ("max_rank_seen", ctypes.c_int),
+        ("factor_bytes", ctypes.c_longlong),
+        ("dense_bytes", ctypes.c_longlong),
+        ("matvec_bytes_per_rhs", ctypes.c_longlong),
+        ("build_seconds", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load libhmb200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libhmb200.so not built: run `make -C %s`" % HERE)
+        L = ctypes.CDLL(LIB_PATH)
+        P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.hm_last_error.restype = ctypes.c_char_p
+        L.hm_version.restype = ctypes.c_char_p
+        L.hm_generate_dataset.argtypes = [I, I, ctypes.c_ulonglong, P, P]
+        L.hm_kdtree_build.argtypes = [P, I, I, I, P, ctypes.POINTER(P)]
+        L.hm_kdtree_info.argtypes = [P, P, P, P, P]
+        L.hm_kdtree_copy_out.argtypes = [P, P, P, P, P, P]
+        L.hm_kdtree_device_perm.argtypes = [P]
+        L.hm_kdtree_device_perm.restype = P
+        L.hm_kdtree_free.argtypes = [P]
+        L.hm_structure_build.argtypes = [P, I, D, P, ctypes.POINTER(P)]
+        L.hm_structure_info.argtypes = [P, P, P]
+        L.hm_structure_tiles.argtypes = [P, I, P]
+        L.hm_structure_jds.argtypes = [P, I, P, P, P, P, P, P]
+        L.hm_structure_free.argtypes = [P]
+        if hasattr(L, "hm_hmatrix_build"):
+            L.hm_build_opts_default.argtypes = [I, ctypes.POINTER(BuildOpts)]
+            L.hm_hmatrix_build.argtypes = [P, P, P, ctypes.POINTER(BuildOpts), P, ctypes.POINTER(P)]
+            L.hm_hmatrix_stats_get.argtypes = [P, ctypes.POINTER(Stats)]
+            L.hm_hmatvec.argtypes = [P, I, I, P, I, P, I, I, P]
+            L.hm_hmatrix_free.argtypes = [P]
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != 0:
+        raise HMError(status, lib().hm_last_error().decode())
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    return ctypes.c_void_p(int(getattr(stream, "cuda_stream", stream)))
+
+
+def version():
+    return lib().hm_version().decode()
+
+
+def generate_dataset(n, d, seed=1234, out=None, stream=None):
+    """Points in SoA layout p[dim*n + i] (float64 CUDA tensor of n*d)."""
+    import torch
+
+    if out is None:
+        out = torch.empty(n * d, dtype=torch.float64, device="cuda")
+    _check(lib().hm_generate_dataset(n, d, seed, _ptr(out), _stream(stream)))
+    return out
+
+
+class KDTree:
+    """Handle of a device KD tree (FULL_TREE division)."""
+
+    def __init__(self, handle):
+        self.h = handle
+        n, d, b, depth = (ctypes.c_int() for _ in range(4))
+        _check(lib().hm_kdtree_info(self.h, ctypes.byref(n), ctypes.byref(d), ctypes.byref(b),
+                                    ctypes.byref(depth)))
+        self.n, self.d, self.bucket, self.depth = n.value, d.value, b.value, depth.value
+
+    def copy_out(self):
+        """Host copies: perm, offsets, bmin, bmax (levels 0..depth), split_dim."""
+        nleaf = 1 << self.depth
+        perm = np.zeros(self.n, np.int32)
+        offs = np.zeros(nleaf + 1, np.int32)
+        bmin = np.zeros((2 * nleaf - 1) * self.d)
+        bmax = np.zeros((2 * nleaf - 1) * self.d)
+        sdim = np.zeros(max(nleaf - 1, 1), np.int32)
+        P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        _check(lib().hm_kdtree_copy_out(self.h, P(perm), P(offs), P(bmin), P(bmax), P(sdim)))
+        return dict(perm=perm, offsets=offs, bmin=bmin, bmax=bmax, split_dim=sdim[: nleaf - 1])
+
+    def free(self):
+        if self.h:
+            lib().hm_kdtree_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def construct_kdtree(points, n, d, bucket, stream=None):
+    h = ctypes.c_void_p()
+    _check(lib().hm_kdtree_build(_ptr(points), n, d, bucket, _stream(stream), ctypes.byref(h)))
+    return KDTree(h)
+
+
+class Structure:
+    def __init__(self, handle, tree):
+        self.h = handle
+        self.tree = tree  # keeps the tree alive
+        nl = ctypes.c_int()
+        _check(lib().hm_structure_info(self.h, ctypes.byref(nl), None))
+        self.num_levels = nl.value
+        self.depth = self.num_levels - 1
+        counts = np.zeros(max(self.depth, 1), np.int32)
+        _check(lib().hm_structure_info(self.h, None, counts.ctypes.data_as(ctypes.c_void_p)))
+        self.counts = counts[: self.depth]
+
+    def tiles(self, level):
+        out = np.zeros(max(int(self.counts[level - 1]), 1), np.int32)
+        _check(lib().hm_structure_tiles(self.h, level, out.ctypes.data_as(ctypes.c_void_p)))
+        return out[: self.counts[level - 1]]
+
+    def all_tiles(self):
+        return [self.tiles(lv) for lv in range(1, self.depth + 1)]
+
+    def jds(self, level):
+        nrows = 1 << level
+        nb = int(self.counts[level - 1])
+        maxc = ctypes.c_int()
+        _check(lib().hm_structure_jds(self.h, level, None, None, None, None, None, ctypes.byref(maxc)))
+        rp = np.zeros(nrows + 1, np.int32)
+        cb = np.zeros(max(nb, 1), np.int32)
+        jr = np.zeros(nrows, np.int32)
+        jp = np.zeros(maxc.value + 1, np.int32)
+        jb = np.zeros(max(nb, 1), np.int32)
+        P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        _check(lib().hm_structure_jds(self.h, level, P(rp), P(cb), P(jr), P(jp), P(jb), None))
+        return dict(row_ptr=rp, csr_blk=cb[:nb], jds_rows=jr, jds_ptr=jp, jds_blk=jb[:nb],
+                    max_row_blocks=maxc.value)
+
+    def free(self):
+        if self.h:
+            lib().hm_structure_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def construct_hmatrix_structure(tree, admissibility=BOX_CENTER, eta=1.0, stream=None):
+    h = ctypes.c_void_p()
+    _check(lib().hm_structure_build(tree.h, admissibility, eta, _stream(stream), ctypes.byref(h)))
+    return Structure(h, tree)
+
+
+# reference-style aliases
+generateDataset = generate_dataset
+constructKDTree = construct_kdtree
+constructHMatrixStructure = construct_hmatrix_structure

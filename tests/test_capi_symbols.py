@@ -1,0 +1,57 @@
+"""The C ABI library loads without a GPU and exports every entry point that
+include/hm.h declares; the oracle library builds and loads."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import PKG, ROOT
+
+HDR = os.path.join(ROOT, "include", "hm.h")
+
+
+def declared_symbols():
+    src = open(HDR).read()
+    return sorted(set(re.findall(r"HM_API\s+[\w\s\*]*?\b(hm_\w+)\s*\(", src)))
+
+
+def test_header_declares_the_pipeline():
+    syms = declared_symbols()
+    for s in ["hm_generate_dataset", "hm_kdtree_build", "hm_structure_build", "hm_hmatrix_build",
+              "hm_hmatvec", "hm_last_error"]:
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    path = os.path.join(PKG, "libhmb200.so")
+    if not os.path.exists(path):
+        pytest.skip("libhmb200.so not built (run __graft_entry__.build())")
+    lib = ctypes.CDLL(path)
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, "not exported: %s" % missing
+
+
+def test_version_and_error_string_without_gpu():
+    path = os.path.join(PKG, "libhmb200.so")
+    if not os.path.exists(path):
+        pytest.skip("libhmb200.so not built")
+    lib = ctypes.CDLL(path)
+    lib.hm_version.restype = ctypes.c_char_p
+    lib.hm_last_error.restype = ctypes.c_char_p
+    assert b"sm_100a" in lib.hm_version()
+    # argument validation happens before any CUDA call
+    lib.hm_kdtree_build.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    out = ctypes.c_void_p()
+    assert lib.hm_kdtree_build(None, 10, 2, 4, None, ctypes.byref(out)) == 1  # HM_ERR_INVALID
+    assert b"NULL" in lib.hm_last_error()
+    assert lib.hm_kdtree_build(ctypes.c_void_p(8), 10, 0, 4, None, ctypes.byref(out)) == 1
+    assert out.value is None
+
+
+def test_oracle_library_loads():
+    import oracle
+
+    assert oracle.tree_depth(8192, 32) == 8
+    assert oracle.morton(1, 0) == 1 and oracle.morton(0, 1) == 2 and oracle.morton(3, 3) == 15
