@@ -171,7 +171,7 @@ typedef struct {
   int max_rank_seen;
   long long factor_bytes;    /* bytes of stored factors */
   long long dense_bytes;     /* bytes of stored dense blocks */
-  long long matvec_bytes_per_rhs; /* unused, 0 */
+  long long num_unconverged; /* blocks above the leaf level left at their rank cap */
   double build_seconds;      /* device time of hm_hmatrix_build */
 } hm_hmatrix_stats;
 
@@ -184,6 +184,27 @@ HM_API hm_status hm_hmatrix_stats_get(hm_hmatrix h, hm_hmatrix_stats* st);
  * host synchronisation: the call is stream-ordered. */
 HM_API hm_status hm_hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, int ldx, float* Y,
                      int ldy, int original_order, void* stream);
+
+/* hm_hmatvec for one panel (nrhs <= the matrix's panel width, 16 by
+ * default), X and Y in tree order, with CUDA events recorded on `stream`
+ * around its two kernels; synchronises and returns each kernel's device time
+ * and algorithmic bytes (stored factors and dense blocks read once, X read,
+ * Y written).  For measurement; the hot path is hm_hmatvec. */
+HM_API hm_status hm_hmatvec_profile(hm_hmatrix h, int nrhs, const float* X, int ldx, float* Y, int ldy,
+                                    void* stream, float* ms_project, float* ms_expand,
+                                    long long* bytes_project, long long* bytes_expand);
+
+/* Block list as the matvec sees it (both orientations of each stored pair),
+ * the counterpart of the reference's HMatrixLevel (src/HMatrix.cuh:9-18).
+ * Any pointer may be NULL.  lowrank: *num_lowrank rows of 6 ints
+ * [r0, m, c0, n, k, level] (tree-order row / column ranges); dense:
+ * *num_dense rows of 5 ints [r0, m, c0, n, transposed]. */
+HM_API hm_status hm_hmatrix_blocks(hm_hmatrix h, long long* num_lowrank, long long* num_dense,
+                                   int* lowrank, int* dense);
+
+/* Host copy of low-rank block i's factors as FP32: U (m x k), V (n x k),
+ * column-major, A_block ~ U V^T. */
+HM_API hm_status hm_hmatrix_block_factors(hm_hmatrix h, int i, float* U, float* V);
 
 HM_API void hm_hmatrix_free(hm_hmatrix h);
 

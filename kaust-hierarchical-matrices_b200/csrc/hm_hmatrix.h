@@ -38,6 +38,7 @@ struct MatvecPlan {
   long long t_per_rhs = 0;   // sum_b k_b
   int nrhs_cap = 0;
   int num_leaves = 0;
+  int maxleaf = 1;
   DevBuf<float> Xp, Yp;      // permuted copies for original-order calls (n * nrhs_cap)
 };
 

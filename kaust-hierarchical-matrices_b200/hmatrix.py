@@ -58,7 +58,7 @@ class Stats(ctypes.Structure):
         ("max_rank_seen", ctypes.c_int),
         ("factor_bytes", ctypes.c_longlong),
         ("dense_bytes", ctypes.c_longlong),
-        ("matvec_bytes_per_rhs", ctypes.c_longlong),
+        ("num_unconverged", ctypes.c_longlong),
         ("build_seconds", ctypes.c_double),
     ]
 
@@ -94,6 +94,8 @@ def lib():
             L.hm_hmatrix_stats_get.argtypes = [P, ctypes.POINTER(Stats)]
             L.hm_hmatvec.argtypes = [P, I, I, P, I, P, I, I, P]
             L.hm_hmatrix_free.argtypes = [P]
+            L.hm_hmatrix_blocks.argtypes = [P, P, P, P, P]
+            L.hm_hmatrix_block_factors.argtypes = [P, I, P, P]
         _lib = L
     return _lib
 
@@ -220,7 +222,100 @@ def construct_hmatrix_structure(tree, admissibility=BOX_CENTER, eta=1.0, stream=
     return Structure(h, tree)
 
 
+class HMatrix:
+    """Handle of a built H-matrix (keeps its tree and structure alive)."""
+
+    def __init__(self, handle, tree, structure):
+        self.h = handle
+        self.tree = tree
+        self.structure = structure
+        self.n = tree.n
+
+    def stats(self):
+        st = Stats()
+        _check(lib().hm_hmatrix_stats_get(self.h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in Stats._fields_}
+
+    def matvec(self, X, Y=None, trans=0, original_order=False, stream=None):
+        """Y = H X for a float32 CUDA tensor X of shape (n, nrhs), column-major
+        (i.e. X.T contiguous) or a contiguous (n,) vector."""
+        import torch
+
+        n = self.n
+        if X.dim() == 1:
+            X = X[:, None]
+        nrhs = X.shape[1]
+        Xc = X.t().contiguous() if not X.t().is_contiguous() else X.t()
+        if Y is None:
+            Yc = torch.empty((nrhs, n), dtype=torch.float32, device=X.device)
+        else:
+            Yc = Y.t()
+            assert Yc.is_contiguous()
+        _check(lib().hm_hmatvec(self.h, trans, nrhs, _ptr(Xc), n, _ptr(Yc), n, 1 if original_order else 0,
+                                _stream(stream)))
+        return Yc.t()
+
+    def blocks(self):
+        """Host copy of the block list: (lowrank rows [r0, m, c0, n, k, level],
+        dense rows [r0, m, c0, n, transposed]), both orientations."""
+        nl, nd = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(lib().hm_hmatrix_blocks(self.h, ctypes.byref(nl), ctypes.byref(nd), None, None))
+        lr = np.zeros((max(nl.value, 1), 6), np.int32)
+        de = np.zeros((max(nd.value, 1), 5), np.int32)
+        _check(lib().hm_hmatrix_blocks(self.h, None, None, lr.ctypes.data_as(ctypes.c_void_p),
+                                       de.ctypes.data_as(ctypes.c_void_p)))
+        return lr[: nl.value], de[: nd.value]
+
+    def block_factors(self, i):
+        """U (m x k) and V (n x k) of low-rank block i, float64 numpy."""
+        lr, _ = self.blocks()
+        r0, m, c0, n, k, lvl = lr[i]
+        U = np.zeros(m * max(k, 1), np.float32)
+        V = np.zeros(n * max(k, 1), np.float32)
+        _check(lib().hm_hmatrix_block_factors(self.h, i, U.ctypes.data_as(ctypes.c_void_p),
+                                              V.ctypes.data_as(ctypes.c_void_p)))
+        return (U[: m * k].reshape(k, m).T.astype(np.float64), V[: n * k].reshape(k, n).T.astype(np.float64))
+
+    def free(self):
+        if self.h:
+            lib().hm_hmatrix_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def default_opts(d):
+    o = BuildOpts()
+    lib().hm_build_opts_default(d, ctypes.byref(o))
+    return o
+
+
+def build_hmatrix(tree, structure, points=None, kernel=K_EXP, ell=None, nugget=0.0, tol=1e-5, max_rank=64,
+                  leaf_max_rank=0, sample_block=16, precision=PREC_FP32, derivative=0, seed=0, stream=None):
+    o = default_opts(tree.d)
+    o.kernel = kernel
+    if ell is not None:
+        o.ell = ell
+    o.nugget = nugget
+    o.tol = tol
+    o.max_rank = max_rank
+    o.leaf_max_rank = leaf_max_rank
+    o.sample_block = sample_block
+    o.precision = precision
+    o.derivative = derivative
+    o.seed = seed
+    h = ctypes.c_void_p()
+    _check(lib().hm_hmatrix_build(tree.h, structure.h, _ptr(points) if points is not None else None,
+                                  ctypes.byref(o), _stream(stream), ctypes.byref(h)))
+    return HMatrix(h, tree, structure)
+
+
 # reference-style aliases
 generateDataset = generate_dataset
 constructKDTree = construct_kdtree
 constructHMatrixStructure = construct_hmatrix_structure
+generateHMatrixFromStruct = build_hmatrix

@@ -301,20 +301,29 @@ static double entry(int kind, int deriv, double ell, double nugget, const double
 int orc_dense_rows_matvec(int n, int d, const double* pts, const int* perm, int kind, int deriv,
                           double ell, double nugget, const int* rows, int nrows, int nrhs,
                           const double* X, double* Y) {
-  double* arow = (double*)malloc(sizeof(double) * (size_t)n);
-  if (!arow) return ORC_ENOMEM;
-  for (int r = 0; r < nrows; ++r) {
-    int pi = perm[rows[r]];
-    for (int j = 0; j < n; ++j) arow[j] = entry(kind, deriv, ell, nugget, pts, n, d, pi, perm[j]);
-    for (int c = 0; c < nrhs; ++c) {
-      double acc = 0;
-      const double* x = X + (size_t)c * n;
-      for (int j = 0; j < n; ++j) acc += arow[j] * x[j];
-      Y[(size_t)c * nrows + r] = acc;
+  int err = 0;
+#pragma omp parallel
+  {
+    double* arow = (double*)malloc(sizeof(double) * (size_t)n);
+    if (!arow) {
+#pragma omp atomic write
+      err = 1;
+    } else {
+#pragma omp for schedule(dynamic, 4)
+      for (int r = 0; r < nrows; ++r) {
+        int pi = perm[rows[r]];
+        for (int j = 0; j < n; ++j) arow[j] = entry(kind, deriv, ell, nugget, pts, n, d, pi, perm[j]);
+        for (int c = 0; c < nrhs; ++c) {
+          double acc = 0;
+          const double* x = X + (size_t)c * n;
+          for (int j = 0; j < n; ++j) acc += arow[j] * x[j];
+          Y[(size_t)c * nrows + r] = acc;
+        }
+      }
+      free(arow);
     }
   }
-  free(arow);
-  return ORC_OK;
+  return err ? ORC_ENOMEM : ORC_OK;
 }
 
 /*

@@ -55,3 +55,26 @@ def test_oracle_library_loads():
 
     assert oracle.tree_depth(8192, 32) == 8
     assert oracle.morton(1, 0) == 1 and oracle.morton(0, 1) == 2 and oracle.morton(3, 3) == 15
+
+
+def test_refcompat_header_compiles(tmp_path):
+    """The reference-name binding (include/hm_refcompat.h) is valid C++ over the C ABI."""
+    import subprocess
+
+    src = tmp_path / "use.cpp"
+    src.write_text('#include "hm_refcompat.h"\n'
+                   'int main() { hmref::KDTree t; hmref::HMatrixStructure s; hmref::HMatrix h;\n'
+                   '  (void)t; (void)s; (void)h; return 0; }\n')
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(src)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_header_is_plain_c(tmp_path):
+    import subprocess
+
+    src = tmp_path / "use.c"
+    src.write_text('#include "hm.h"\nint main(void) { hm_build_opts o; (void)o; return 0; }\n')
+    r = subprocess.run(["gcc", "-std=c99", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(src)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

@@ -1,0 +1,174 @@
+"""H-matrix build and H-matvec on the GPU through the C ABI, against the FP64
+CPU oracle: every compressed block meets ||A - U V^T||_F / ||A||_F <= tol
+(src/expandMatrix.cu:31-37,66-97), and the product's relative error against a
+dense FP64 product (src/expandMatrix.cu:221-231) is stated and bounded."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def hm():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import hmatrix
+
+    return hmatrix
+
+
+def build(hm, n, d, b, kernel, ell, tol, max_rank, adm=1, eta=1.0, nugget=0.0, seed=1234, deriv=0,
+          points=None, sample_block=16):
+    import torch
+
+    if points is None:
+        pts = hm.generate_dataset(n, d, seed=seed)
+    else:
+        pts = torch.from_numpy(np.ascontiguousarray(points, dtype=np.float64)).cuda()
+    tree = hm.construct_kdtree(pts, n, d, b)
+    st = hm.construct_hmatrix_structure(tree, adm, eta)
+    H = hm.build_hmatrix(tree, st, pts, kernel=kernel, ell=ell, nugget=nugget, tol=tol, max_rank=max_rank,
+                         derivative=deriv, sample_block=sample_block)
+    return pts.cpu().numpy(), tree, st, H
+
+
+def check_blocks(H, pts, n, d, perm, kind, ell, nugget, tol, deriv=0, max_blocks=None, seed=0):
+    lr, de = H.blocks()
+    idx = np.arange(len(lr))
+    # one orientation of each stored pair suffices (the mirror shares factors)
+    idx = idx[lr[idx, 0] > lr[idx, 2]]
+    if max_blocks is not None and len(idx) > max_blocks:
+        idx = np.random.default_rng(seed).choice(idx, max_blocks, replace=False)
+    worst = 0.0
+    for i in idx:
+        r0, m, c0, nn, k, lvl = lr[i]
+        U, V = H.block_factors(int(i))
+        err = oracle.block_error(pts, n, d, perm, kind, ell, nugget, int(r0), int(m), int(c0), int(nn), U, V,
+                                 deriv=deriv)
+        worst = max(worst, err)
+        assert err <= tol, "block %d (r0=%d m=%d c0=%d n=%d k=%d level=%d): %g > %g" % (
+            i, r0, m, c0, nn, k, lvl, err, tol)
+    return worst
+
+
+def check_cover(H, n):
+    lr, de = H.blocks()
+    # every (leaf-row, leaf-col) region covered exactly once: count entries
+    area = 0
+    for r0, m, c0, nn, *_ in lr:
+        area += int(m) * int(nn)
+    for r0, m, c0, nn, _ in de:
+        area += int(m) * int(nn)
+    assert area == n * n
+
+
+def test_c1_plain_fp32_build_and_matvec(hm):
+    """The small plain-FP32 workload: N=8192 uniform 2-D points from the
+    reference's generator, exp(-r/0.1), bucket 32, box-center eta=1, tol 1e-6,
+    sample block 16, max rank 64."""
+    import torch
+
+    n, d, b, tol = 8192, 2, 32, 1e-6
+    pts, tree, st, H = build(hm, n, d, b, hm.K_EXP, 0.1, tol, 64)
+    perm = tree.copy_out()["perm"]
+    s = H.stats()
+    assert s["num_unconverged"] == 0
+    check_cover(H, n)
+    worst = check_blocks(H, pts, n, d, perm, oracle.K_EXP, 0.1, 0.0, tol)
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(n)
+    y = H.matvec(torch.from_numpy(x.astype(np.float32)).cuda()).cpu().numpy()[:, 0]
+    yref = oracle.dense_rows_matvec(pts, n, d, perm, oracle.K_EXP, 0.1, 0.0, np.arange(n), x)[0]
+    err = np.linalg.norm(y - yref) / np.linalg.norm(yref)
+    print("C1: worst block error %.3g, matvec rel err %.3g, stats %s" % (worst, err, s))
+    assert err < 2e-5
+
+
+@pytest.mark.parametrize("kind,ell,nugget,tol,d,b", [
+    (1, 0.2, 1e-3, 1e-4, 3, 64),   # Matern-3/2 + nugget, the precision-form kernel
+    (2, 0.15, 0.0, 1e-6, 3, 64),   # Gaussian, the differentiation-form kernel
+    (0, 0.05, 0.0, 1e-4, 3, 32),   # short exponential, the scale-stress kernel
+])
+def test_kernels_block_tolerance(hm, kind, ell, nugget, tol, d, b):
+    import torch
+
+    n = 20000
+    pts, tree, st, H = build(hm, n, d, b, kind, ell, tol, 128 if tol >= 1e-4 else 96, nugget=nugget, seed=77)
+    perm = tree.copy_out()["perm"]
+    assert H.stats()["num_unconverged"] == 0
+    check_cover(H, n)
+    check_blocks(H, pts, n, d, perm, kind, ell, nugget, tol, max_blocks=400)
+    rng = np.random.default_rng(2)
+    X = rng.standard_normal((n, 3))
+    Y = H.matvec(torch.from_numpy(X.astype(np.float32)).cuda()).cpu().numpy()
+    rows = rng.choice(n, 500, replace=False)
+    Yref = oracle.dense_rows_matvec(pts, n, d, perm, kind, ell, nugget, rows, X.T).T
+    err = np.linalg.norm(Y[rows] - Yref) / np.linalg.norm(Yref)
+    assert err < max(20 * tol, 5e-6), err
+
+
+def test_derivative_kernel_blocks(hm):
+    n, d, b, tol, ell = 12000, 3, 64, 1e-6, 0.15
+    pts, tree, st, H = build(hm, n, d, b, hm.K_GAUSS, ell, tol, 96, deriv=1, seed=5)
+    perm = tree.copy_out()["perm"]
+    check_blocks(H, pts, n, d, perm, oracle.K_GAUSS, ell, 0.0, tol, deriv=1, max_blocks=300)
+
+
+def test_matvec_orders_transpose_and_panels(hm):
+    import torch
+
+    n, d, b = 10000, 3, 32
+    pts, tree, st, H = build(hm, n, d, b, hm.K_EXP, 0.2, 1e-5, 64, seed=3)
+    perm = tree.copy_out()["perm"]
+    rng = np.random.default_rng(4)
+    X = rng.standard_normal((n, 40)).astype(np.float32)  # more than one rhs panel
+    Xd = torch.from_numpy(X).cuda()
+    Y = H.matvec(Xd).cpu().numpy()
+    # each column independently
+    for c in (0, 17, 39):
+        yc = H.matvec(Xd[:, c].contiguous()).cpu().numpy()[:, 0]
+        np.testing.assert_allclose(yc, Y[:, c], rtol=1e-5, atol=1e-5 * np.abs(Y[:, c]).max())
+    # the operator is symmetric: H^T X == H X exactly
+    Yt = H.matvec(Xd, trans=1).cpu().numpy()
+    np.testing.assert_array_equal(Yt, Y)
+    # original order: Y_orig[perm] = H (X_orig[perm])
+    Xo = np.empty_like(X)
+    Xo[perm] = X
+    Yo = H.matvec(torch.from_numpy(Xo).cuda(), original_order=True).cpu().numpy()
+    np.testing.assert_allclose(Yo[perm], Y, rtol=1e-6, atol=1e-6 * np.abs(Y).max())
+    # linearity
+    Y2 = H.matvec(torch.from_numpy(2.0 * X[:, :5] - X[:, 5:10]).cuda()).cpu().numpy()
+    np.testing.assert_allclose(Y2, 2 * Y[:, :5] - Y[:, 5:10], rtol=1e-4, atol=1e-4 * np.abs(Y).max())
+
+
+def test_weak_admissibility_and_odd_sizes(hm):
+    import torch
+
+    for n, d, b in [(3000, 2, 32), (777, 1, 16), (20, 2, 32), (5000, 3, 64)]:
+        pts, tree, st, H = build(hm, n, d, b, hm.K_EXP, 0.1, 1e-6, 64, adm=0, seed=n)
+        perm = tree.copy_out()["perm"]
+        check_cover(H, n)
+        x = np.random.default_rng(n).standard_normal(n)
+        y = H.matvec(torch.from_numpy(x.astype(np.float32)).cuda()).cpu().numpy()[:, 0]
+        yref = oracle.dense_rows_matvec(pts, n, d, perm, oracle.K_EXP, 0.1, 0.0, np.arange(n), x)[0]
+        assert np.linalg.norm(y - yref) / np.linalg.norm(yref) < 2e-5
+
+
+def test_rejects_bad_options(hm):
+    import ctypes
+
+    pts = hm.generate_dataset(1000, 2)
+    tree = hm.construct_kdtree(pts, 1000, 2, 32)
+    st = hm.construct_hmatrix_structure(tree)
+    with pytest.raises(hm.HMError):
+        hm.build_hmatrix(tree, st, pts, tol=0.0)
+    with pytest.raises(hm.HMError):
+        hm.build_hmatrix(tree, st, pts, kernel=7)
+    with pytest.raises(hm.HMError):
+        hm.build_hmatrix(tree, st, pts, max_rank=200)
+    with pytest.raises(hm.HMError):
+        hm.build_hmatrix(tree, st, pts, sample_block=64)
