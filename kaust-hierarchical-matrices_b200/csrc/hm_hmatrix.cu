@@ -412,11 +412,17 @@ __global__ void __launch_bounds__(kOrthThreads) k_orth(OrthArgs<W> a) {
     return;
   }
   apply_linv(Y, m, bs, Gs, perm, r);
-  // two Cholesky-QR refinements of the r kept columns
+  // Refinements.  R^{-1} of an ill-conditioned sample magnifies whatever the
+  // Gram-Schmidt left along the old basis, so after the first refinement the
+  // block is projected against Q once more before the final Cholesky-QR.
   for (int pass = 0; pass < 2 && r > 0; ++pass) {
+    if (pass == 1 && k > 0) {
+      block_qty(Q, Y, m, k, r, Csm, stage);
+      block_update(Q, Y, m, k, r, Csm);
+    }
     const int rg = r;  // dimension (and row stride) of this Gram matrix
     gram64(Y, m, rg, Gs, stage);
-    if (threadIdx.x == 0) rank_sh = chol_pivoted(Gs, rg, perm, false, 0.0);
+    if (threadIdx.x == 0) rank_sh = chol_pivoted(Gs, rg, perm, pass == 1, pass == 1 ? 1e-12 * rg : 0.0);
     __syncthreads();
     r = rank_sh;  // a refinement that loses rank keeps the leading columns
     if (r > 0) apply_linv(Y, m, rg, Gs, perm, r);

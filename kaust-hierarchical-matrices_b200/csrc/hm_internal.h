@@ -33,21 +33,31 @@ hm_status cuda_fail(cudaError_t e, const char* what, const char* file, int line)
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // ---- device buffer RAII -----------------------------------------------------
+// Long-lived buffers use cudaMalloc; temporaries of a build step pass a stream
+// and come from the stream-ordered pool (cudaMallocAsync / cudaFreeAsync), so
+// freeing them neither synchronises the device nor returns memory to the OS.
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  cudaStream_t s = nullptr;
+  bool async = false;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), s(o.s), async(o.async) { o.p = nullptr; o.n = 0; }
   DevBuf& operator=(DevBuf&& o) noexcept {
-    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    if (this != &o) {
+      release();
+      p = o.p; n = o.n; s = o.s; async = o.async;
+      o.p = nullptr; o.n = 0;
+    }
     return *this;
   }
   ~DevBuf() { release(); }
   hm_status alloc(size_t count) {
     release();
+    async = false;
     if (count == 0) return HM_OK;
     cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
     if (e != cudaSuccess) {
@@ -59,8 +69,26 @@ struct DevBuf {
     n = count;
     return HM_OK;
   }
+  hm_status alloc_async(size_t count, cudaStream_t stream) {
+    release();
+    async = true;
+    s = stream;
+    if (count == 0) return HM_OK;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), stream);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      return fail(HM_ERR_NOMEM, "cudaMallocAsync of " + std::to_string(count * sizeof(T)) +
+                                    " bytes failed: " + cudaGetErrorString(e));
+    }
+    n = count;
+    return HM_OK;
+  }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (async) cudaFreeAsync(p, s);
+      else cudaFree(p);
+    }
     p = nullptr;
     n = 0;
   }

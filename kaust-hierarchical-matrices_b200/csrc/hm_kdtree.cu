@@ -649,8 +649,8 @@ hm_status kdtree_build(const double* d_points, int n, int d, int bucket, cudaStr
 
   DevBuf<int> idxA, idxB;
   DevBuf<double> coA, coB;
-  if ((s = idxA.alloc(n)) || (s = idxB.alloc(n)) || (s = coA.alloc((size_t)d * n)) ||
-      (s = coB.alloc((size_t)d * n)))
+  if ((s = idxA.alloc_async(n, stream)) || (s = idxB.alloc_async(n, stream)) || (s = coA.alloc_async((size_t)d * n, stream)) ||
+      (s = coB.alloc_async((size_t)d * n, stream)))
     return cleanup(s);
   auto cu = [&](cudaError_t e, const char* what) -> hm_status {
     if (e != cudaSuccess) return cuda_fail(e, what, __FILE__, __LINE__);

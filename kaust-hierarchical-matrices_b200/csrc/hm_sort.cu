@@ -113,9 +113,9 @@ hm_status sort_pairs_u32(uint32_t* keys, uint32_t* vals, int n, int key_bits, cu
   int ntiles = (n + kTile - 1) / kTile;
   DevBuf<uint32_t> k2, v2;
   DevBuf<unsigned int> hist;
-  HM_TRY(k2.alloc(n));
-  HM_TRY(v2.alloc(n));
-  HM_TRY(hist.alloc((size_t)256 * ntiles));
+  HM_TRY(k2.alloc_async(n, stream));
+  HM_TRY(v2.alloc_async(n, stream));
+  HM_TRY(hist.alloc_async((size_t)256 * ntiles, stream));
   uint32_t *ka = keys, *va = vals, *kb = k2.p, *vb = v2.p;
   int passes = 0;
   for (int shift = 0; shift < key_bits; shift += 8) {
@@ -132,9 +132,7 @@ hm_status sort_pairs_u32(uint32_t* keys, uint32_t* vals, int n, int key_bits, cu
     HM_CUDA(cudaMemcpyAsync(keys, ka, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, stream));
     HM_CUDA(cudaMemcpyAsync(vals, va, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, stream));
   }
-  // temporaries are released at return: wait for the device to finish with them
-  HM_CUDA(cudaStreamSynchronize(stream));
-  return HM_OK;
+  return HM_OK;  // temporaries are released in stream order
 }
 
 }  // namespace hm

@@ -199,7 +199,7 @@ hm_status structure_build(hm_kdtree t, int admiss, double eta, cudaStream_t stre
   DevBuf<uint32_t> front, next;
   DevBuf<unsigned int> crec, cref;
   hm_status st;
-  if ((st = front.alloc(1))) return cleanup(st);
+  if ((st = front.alloc_async(1, stream))) return cleanup(st);
   uint32_t zero = 0;
   HM_CUDA(cudaMemcpyAsync(front.p, &zero, 4, cudaMemcpyHostToDevice, stream));
   long long nf = 1;
@@ -215,7 +215,7 @@ hm_status structure_build(hm_kdtree t, int admiss, double eta, cudaStream_t stre
     a.bmin = t->bmin.p;
     a.bmax = t->bmax.p;
     int nb = (int)((nf + kThreads - 1) / kThreads);
-    if ((st = crec.alloc(nb)) || (st = cref.alloc(nb))) return cleanup(st);
+    if ((st = crec.alloc_async(nb, stream)) || (st = cref.alloc_async(nb, stream))) return cleanup(st);
     k_classify_count<<<nb, kThreads, 0, stream>>>(a, crec.p, cref.p);
     HM_LAUNCH_CHECK();
     std::vector<unsigned int> hr(nb), hf(nb);
@@ -235,9 +235,9 @@ hm_status structure_build(hm_kdtree t, int admiss, double eta, cudaStream_t stre
     HM_CUDA(cudaMemcpyAsync(cref.p, hf.data(), 4 * nb, cudaMemcpyHostToDevice, stream));
     DevBuf<uint32_t> rec;
     if (level >= 1 && trec > 0) {
-      if ((st = rec.alloc(trec))) return cleanup(st);
+      if ((st = rec.alloc_async(trec, stream))) return cleanup(st);
     }
-    if ((st = next.alloc(std::max<unsigned long long>(4 * tref, 1)))) return cleanup(st);
+    if ((st = next.alloc_async(std::max<unsigned long long>(4 * tref, 1), stream))) return cleanup(st);
     k_classify_scatter<<<nb, kThreads, 0, stream>>>(a, crec.p, cref.p, rec.p, next.p);
     HM_LAUNCH_CHECK();
     HM_CUDA(cudaStreamSynchronize(stream));
@@ -293,7 +293,7 @@ hm_status structure_build(hm_kdtree t, int admiss, double eta, cudaStream_t stre
       continue;
     }
     DevBuf<uint32_t> keys, vals;
-    if ((st = keys.alloc(std::max(nb, nrows))) || (st = vals.alloc(std::max(nb, nrows))))
+    if ((st = keys.alloc_async(std::max(nb, nrows), stream)) || (st = vals.alloc_async(std::max(nb, nrows), stream)))
       return cleanup(st);
     k_row_keys<<<(nb + 255) / 256, 256, 0, stream>>>(s->tiles.p + s->start[l - 1], nb, keys.p, vals.p,
                                                      rp);
@@ -312,7 +312,7 @@ hm_status structure_build(hm_kdtree t, int admiss, double eta, cudaStream_t stre
     if ((st = sort_pairs_u32(keys.p, vals.p, nrows, ceil_log2(maxc + 1), stream))) return cleanup(st);
     HM_CUDA(cudaMemcpyAsync(rows, vals.p, 4 * (size_t)nrows, cudaMemcpyDeviceToDevice, stream));
     DevBuf<unsigned int> dlen;
-    if ((st = dlen.alloc(maxc + 1))) return cleanup(st);
+    if ((st = dlen.alloc_async(maxc + 1, stream))) return cleanup(st);
     HM_CUDA(cudaMemsetAsync(dlen.p, 0, 4 * (size_t)(maxc + 1), stream));
     k_diag_count<<<(nrows + 255) / 256, 256, 0, stream>>>(rp, nrows, dlen.p);
     HM_LAUNCH_CHECK();

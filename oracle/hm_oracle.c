@@ -359,6 +359,22 @@ double orc_block_error(int n, int d, const double* pts, const int* perm, int kin
   return den > 0 ? sqrt(num / den) : sqrt(num);
 }
 
+/*
+ * Rows `rows[0..nrows)` (tree-order indices) of the kernel matrix restricted to
+ * columns [c0, c0+ncols): out is nrows x ncols, row-major.  Used to check
+ * sampled rows of large blocks.
+ */
+int orc_dense_rows_block(int n, int d, const double* pts, const int* perm, int kind, int deriv,
+                         double ell, double nugget, const int* rows, int nrows, int c0, int ncols,
+                         double* out) {
+#pragma omp parallel for schedule(static)
+  for (int r = 0; r < nrows; ++r)
+    for (int j = 0; j < ncols; ++j)
+      out[(size_t)r * ncols + j] =
+          entry(kind, deriv, ell, nugget, pts, n, d, perm[rows[r]], perm[c0 + j]);
+  return ORC_OK;
+}
+
 /* Relative error ||y - y_ref|| / ||y_ref|| (src/expandMatrix.cu:221-231). */
 double orc_rel_error(const double* y, const double* yref, long long len) {
   double num = 0, den = 0;

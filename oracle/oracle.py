@@ -35,6 +35,7 @@ def lib():
         L.orc_block_error.restype = dbl
         L.orc_kernel_r2.argtypes = [i, i, dbl, dbl]
         L.orc_kernel_r2.restype = dbl
+        L.orc_dense_rows_block.argtypes = [i, i, P, P, i, i, dbl, dbl, P, i, i, i, P]
         L.orc_morton.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
         L.orc_morton.restype = ctypes.c_uint32
         L.orc_blas_open.argtypes = [ctypes.c_char_p, i]
@@ -114,6 +115,16 @@ def dense_block(points, n, d, perm, kind, ell, nugget, r0, m, c0, ncols, deriv=0
     lib().orc_dense_block(n, d, _p(pts), _p(np.ascontiguousarray(perm, np.int32)), kind, deriv, ell,
                           nugget, r0, m, c0, ncols, _p(out))
     return out.T  # (m, ncols)
+
+
+def dense_rows_block(points, n, d, perm, kind, ell, nugget, rows, c0, ncols, deriv=0):
+    """A[rows, c0:c0+ncols] in FP64 (rows: tree-order indices); shape (len(rows), ncols)."""
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1)
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    out = np.zeros((len(rows), ncols))
+    lib().orc_dense_rows_block(n, d, _p(pts), _p(np.ascontiguousarray(perm, np.int32)), kind, deriv, ell, nugget,
+                               _p(rows), len(rows), c0, ncols, _p(out))
+    return out
 
 
 def block_error(points, n, d, perm, kind, ell, nugget, r0, m, c0, ncols, U, V, deriv=0):

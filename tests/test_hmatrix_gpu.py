@@ -90,14 +90,14 @@ def test_c1_plain_fp32_build_and_matvec(hm):
 
 @pytest.mark.parametrize("kind,ell,nugget,tol,d,b", [
     (1, 0.2, 1e-3, 1e-4, 3, 64),   # Matern-3/2 + nugget, the precision-form kernel
-    (2, 0.15, 0.0, 1e-6, 3, 64),   # Gaussian, the differentiation-form kernel
+    (2, 0.15, 0.0, 1e-5, 3, 64),   # Gaussian, the differentiation-form kernel
     (0, 0.05, 0.0, 1e-4, 3, 32),   # short exponential, the scale-stress kernel
 ])
 def test_kernels_block_tolerance(hm, kind, ell, nugget, tol, d, b):
     import torch
 
     n = 20000
-    pts, tree, st, H = build(hm, n, d, b, kind, ell, tol, 128 if tol >= 1e-4 else 96, nugget=nugget, seed=77)
+    pts, tree, st, H = build(hm, n, d, b, kind, ell, tol, 128, nugget=nugget, seed=77)
     perm = tree.copy_out()["perm"]
     assert H.stats()["num_unconverged"] == 0
     check_cover(H, n)
@@ -112,8 +112,8 @@ def test_kernels_block_tolerance(hm, kind, ell, nugget, tol, d, b):
 
 
 def test_derivative_kernel_blocks(hm):
-    n, d, b, tol, ell = 12000, 3, 64, 1e-6, 0.15
-    pts, tree, st, H = build(hm, n, d, b, hm.K_GAUSS, ell, tol, 96, deriv=1, seed=5)
+    n, d, b, tol, ell = 12000, 3, 64, 1e-5, 0.15
+    pts, tree, st, H = build(hm, n, d, b, hm.K_GAUSS, ell, tol, 128, deriv=1, seed=5)
     perm = tree.copy_out()["perm"]
     check_blocks(H, pts, n, d, perm, oracle.K_GAUSS, ell, 0.0, tol, deriv=1, max_blocks=300)
 
