@@ -185,6 +185,26 @@ HM_API hm_status hm_hmatrix_stats_get(hm_hmatrix h, hm_hmatrix_stats* st);
 HM_API hm_status hm_hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, int ldx, float* Y,
                      int ldy, int original_order, void* stream);
 
+/* Allocation-free product.  No counterpart in the reference.
+ *
+ * Same result as hm_hmatvec(h, 0, nrhs, X, ldx, Y, ldy, 0, stream) (tree
+ * order), for callers that may not allocate device memory when they apply the
+ * operator -- code running under an external allocator that owns all device
+ * memory, or a latency-bound loop in which a cudaMalloc (which can synchronise
+ * the device) is not acceptable.  It allocates nothing and does not use the
+ * matrix's own projection workspace: its scratch is one fixed 16 MiB array in
+ * the library's device image, held by every GPU that loads the library until
+ * the process exits.  Matrices whose projections need more than that
+ * (sum of ranks x 16 floats > 4 Mi) are rejected with HM_ERR_UNSUPPORTED.
+ *
+ * The first call on a device resolves the array's device address on that
+ * device (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  All calls on a device share the one array and clear the part
+ * they use before the product: calls whose work overlaps on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller. */
+HM_API hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, int ldx, float* Y, int ldy,
+                                    void* stream);
+
 /* hm_hmatvec for one panel (nrhs <= the matrix's panel width, 16 by
  * default), X and Y in tree order, with CUDA events recorded on `stream`
  * around its two kernels; synchronises and returns each kernel's device time

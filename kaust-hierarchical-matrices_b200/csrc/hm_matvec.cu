@@ -16,10 +16,18 @@
 // Both launches are stream ordered and allocation free; X/Y in the points'
 // original order are gathered / scattered through the tree permutation.
 #include <algorithm>
+#include <mutex>
 #include <numeric>
 
 #include "hm_hmatrix.h"
 #include "hm_structure.h"
+
+// Scratch of the allocation-free product (hm_hmatvec_noalloc): 4 Mi floats
+// (16 MiB) in the library's device image.  Every GPU that loads the library
+// holds this array until the process exits.  Host code must not take its
+// address directly (on the host the name is only a stand-in); the device
+// address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) float hm_noalloc_scratch[size_t(4) << 20];
 
 namespace hm {
 namespace {
@@ -380,6 +388,71 @@ extern "C" hm_status hm_hmatvec_profile(hm_hmatrix h, int nrhs, const float* X, 
   hm::matvec_bytes(h, nrhs, &bp, &be);
   if (bytes_project) *bytes_project = bp;
   if (bytes_expand) *bytes_expand = be;
+  return HM_OK;
+}
+
+namespace hm {
+namespace {
+
+constexpr size_t kNoallocScratchFloats = size_t(4) << 20;
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+float* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the static scratch on the current device, resolved on the
+// first call for that device.
+hm_status noalloc_scratch(float** out) {
+  int dev = 0;
+  HM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(HM_ERR_UNSUPPORTED, "hm_hmatvec_noalloc: device ordinal >= 64");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, hm_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(hm_noalloc_scratch)", __FILE__, __LINE__);
+    g_noalloc_ptr[dev] = static_cast<float*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return HM_OK;
+}
+
+}  // namespace
+}  // namespace hm
+
+// The product of hm_hmatvec (tree order) with its projection workspace taken
+// from the library's static scratch instead of the matrix's own buffer; no
+// allocation of any kind.
+extern "C" hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, int ldx, float* Y, int ldy,
+                                        void* stream) {
+  if (!h) return hm::fail(HM_ERR_INVALID, "hm_hmatvec_noalloc: null matrix");
+  if (nrhs < 1 || !X || !Y || ldx < h->n || ldy < h->n)
+    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_noalloc: bad vector arguments");
+  hm::MatvecPlan& P = h->plan;
+  const size_t need = (size_t)P.t_per_rhs * (size_t)P.nrhs_cap;
+  if (need > hm::kNoallocScratchFloats)
+    return hm::fail(HM_ERR_UNSUPPORTED,
+                    "hm_hmatvec_noalloc: this matrix needs " + std::to_string(need) +
+                        " floats of projection scratch (sum of ranks x panel width); the static scratch holds " +
+                        std::to_string(hm::kNoallocScratchFloats) + " (16 MiB)");
+  float* T = nullptr;
+  HM_TRY(hm::noalloc_scratch(&T));
+  cudaStream_t s = hm::as_stream(stream);
+  for (int c0 = 0; c0 < nrhs; c0 += P.nrhs_cap) {
+    const int nr = std::min(P.nrhs_cap, nrhs - c0);
+    const float* Xin = X + (size_t)c0 * ldx;
+    float* Yout = Y + (size_t)c0 * ldy;
+    // the scratch keeps the previous call's contents: the projections must start at zero
+    if (need > 0) HM_CUDA(cudaMemsetAsync(T, 0, sizeof(float) * need, s));
+    if (P.num_p1 > 0) {
+      hm::k_mv_project<<<P.num_p1, hm::kThreads, sizeof(float) * (hm::kMaxK * 33 + 32 * 33), s>>>(
+          reinterpret_cast<const int2*>(P.p1_items.p), P.lr.p, Xin, ldx, nr, T);
+      HM_LAUNCH_CHECK();
+    }
+    hm::k_mv_expand<<<P.num_leaves, hm::kThreads, hm::expand_smem(P.maxleaf, nr), s>>>(
+        h->tree->offsets.p, P.leaf_ptr.p, P.leaf_blk.p, P.lr.p, P.leaf_dptr.p, P.leaf_dblk.p, P.dense.p, T, Xin,
+        ldx, Yout, ldy, nr);
+    HM_LAUNCH_CHECK();
+  }
   return HM_OK;
 }
 
