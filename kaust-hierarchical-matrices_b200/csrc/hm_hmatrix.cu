@@ -27,8 +27,10 @@
 #include <cmath>
 #include <cstdio>
 #include <numeric>
+#include <type_traits>
 
 #include "hm_hmatrix.h"
+#include "hm_mma.cuh"
 #include "hm_structure.h"
 
 namespace hm {
@@ -59,6 +61,8 @@ struct ProbState {
   int active;
   int converged;
   int rounds;
+  int r;      // rank after truncation (<= k)
+  int pad;
 };
 
 template <typename W>
@@ -191,6 +195,170 @@ __global__ void __launch_bounds__(kKmmThreads) k_kmm(KmmArgs<W> a) {
       for (int w = 0; w < kKmmThreads / 32; ++w) tot += red[w];
       atomicAdd(&a.st[it.x].normA2, tot);
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_kmm_tc: the same product on the tensor cores (FP32 working precision).
+// CTA = 4 warps = 64 operator rows, warp = 16 rows; each lane evaluates the
+// eight kernel entries of its m16n8k16 A fragment in registers and splits
+// them into BF16 hi + lo (relative error ~2^-17 of an entry).  Sample pass:
+// W = a Gaussian table whose entries are BF16 numbers, 2 MMAs per tile.
+// Projection pass: W = Q split hi + lo, 3 MMAs per tile (hi*hi, lo*hi, hi*lo).
+// ---------------------------------------------------------------------------
+constexpr int kWS = 136;  // word stride of the staged W pairs (== 8 mod 32: conflict-free fragments)
+
+struct KmmTcArgs {
+  const Prob* probs;
+  ProbState* st;
+  const int2* items;
+  const float* pts;
+  int npts, d;
+  KernelParams kp;
+  int mode;      // 0 sample (bs columns of the Gaussian table), 1 projection (k columns of Q)
+  int bs;
+  int round;
+  const float* omega;  // Gaussian table, [max columns][bs], BF16-exact values
+  int omega_rows;
+  float* ws;
+};
+
+__device__ __forceinline__ float kentry(const KernelParams& kp, const float* rc, const float* cc, int d) {
+  float r2 = 0.f;
+  for (int k = 0; k < d; ++k) {
+    float df = rc[k] - cc[k * kTC];
+    r2 = fmaf(df, df, r2);
+  }
+  return kernel_r2(kp, r2);
+}
+
+__global__ void __launch_bounds__(128) k_kmm_tc(KmmTcArgs a) {
+  __shared__ float colc[kMaxDim * kTC];
+  __shared__ uint32_t Whi[(kTC / 2) * kWS];
+  __shared__ uint32_t Wlo[(kTC / 2) * kWS];
+  __shared__ double red[4];
+  const int2 it = a.items[blockIdx.x];
+  const Prob P = a.probs[it.x];
+  const ProbState S = a.st[it.x];
+  if (a.mode == 0 && !S.active) return;
+  const int s = a.mode == 0 ? a.bs : S.k;
+  if (s <= 0) return;
+  const int mr = a.mode ? P.n : P.m;
+  const int nc = a.mode ? P.m : P.n;
+  const int rbase = a.mode ? P.c0 : P.r0;
+  const int cbase = a.mode ? P.r0 : P.c0;
+  float* out = a.ws + (a.mode ? P.boff : P.yoff);
+  const float* Q = a.ws + P.qoff;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int ra = it.y * kTR + warp * 16 + g, rb = ra + 8;
+  const bool ra_ok = ra < mr, rb_ok = rb < mr;
+  float rca[kMaxDim], rcb[kMaxDim];
+#pragma unroll
+  for (int k = 0; k < kMaxDim; ++k) {
+    rca[k] = (k < a.d && ra_ok) ? a.pts[(size_t)k * a.npts + rbase + ra] : 0.f;
+    rcb[k] = (k < a.d && rb_ok) ? a.pts[(size_t)k * a.npts + rbase + rb] : 0.f;
+  }
+  const int ntiles = (s + 7) >> 3;
+  float acc[16][4];
+#pragma unroll
+  for (int nt = 0; nt < 16; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+  float nrm = 0.f;
+  const bool want_norm = a.mode == 0 && a.round == 0;
+  for (int c0 = 0; c0 < nc; c0 += kTC) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < a.d * kTC; e += blockDim.x) {
+      int k = e / kTC, jj = e % kTC;
+      colc[e] = c0 + jj < nc ? a.pts[(size_t)k * a.npts + cbase + c0 + jj] : 0.f;
+    }
+    // W pairs along the column index: word (jp, n) = {W[2jp][n], W[2jp+1][n]}
+    for (int e = threadIdx.x; e < (kTC / 2) * s; e += blockDim.x) {
+      int n = e / (kTC / 2), jp = e % (kTC / 2);
+      int j0 = c0 + 2 * jp;
+      float w0 = 0.f, w1 = 0.f;
+      if (a.mode == 0) {
+        if (j0 < nc) w0 = a.omega[(size_t)j0 * a.bs + n];
+        if (j0 + 1 < nc) w1 = a.omega[(size_t)(j0 + 1) * a.bs + n];
+        Whi[jp * kWS + n] = pack_bf16(w0, w1);
+      } else {
+        if (j0 < nc) w0 = Q[(size_t)n * P.m + j0];
+        if (j0 + 1 < nc) w1 = Q[(size_t)n * P.m + j0 + 1];
+        uint32_t hi, lo;
+        split_bf16x2(w0, w1, hi, lo);
+        Whi[jp * kWS + n] = hi;
+        Wlo[jp * kWS + n] = lo;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ks = 0; ks < kTC / 16; ++ks) {
+      const int cb = ks * 16 + 2 * t;  // columns cb, cb+1, cb+8, cb+9 of the chunk
+      float e[8];
+      const int cols[4] = {cb, cb + 1, cb + 8, cb + 9};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const bool cok = c0 + cols[q] < nc;
+        e[q] = (ra_ok && cok) ? kentry(a.kp, rca, colc + cols[q], a.d) : 0.f;
+        e[4 + q] = (rb_ok && cok) ? kentry(a.kp, rcb, colc + cols[q], a.d) : 0.f;
+      }
+      if (want_norm) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) nrm = fmaf(e[q], e[q], nrm);
+      }
+      uint32_t ah[4], al[4];
+      split_bf16x2(e[0], e[1], ah[0], al[0]);  // row g, cols cb, cb+1
+      split_bf16x2(e[4], e[5], ah[1], al[1]);  // row g+8
+      split_bf16x2(e[2], e[3], ah[2], al[2]);  // row g, cols cb+8, cb+9
+      split_bf16x2(e[6], e[7], ah[3], al[3]);  // row g+8
+      const int wrow = ks * 8 + t;
+#pragma unroll
+      for (int nt = 0; nt < 16; ++nt) {
+        if (nt < ntiles) {
+          const int n = nt * 8 + g;
+          uint32_t b0 = Whi[wrow * kWS + n], b1 = Whi[(wrow + 4) * kWS + n];
+          float dacc[4] = {0.f, 0.f, 0.f, 0.f};
+          if (a.mode == 1) {
+            uint32_t l0 = Wlo[wrow * kWS + n], l1 = Wlo[(wrow + 4) * kWS + n];
+            mma_bf16(dacc, ah[0], ah[1], ah[2], ah[3], l0, l1);
+          }
+          mma_bf16(dacc, al[0], al[1], al[2], al[3], b0, b1);
+          mma_bf16(dacc, ah[0], ah[1], ah[2], ah[3], b0, b1);
+          add4(acc[nt], dacc);  // round-to-nearest accumulation across k-steps
+        }
+      }
+    }
+  }
+  const int ld = mr;
+#pragma unroll
+  for (int nt = 0; nt < 16; ++nt) {
+    if (nt < ntiles) {
+      const int c = nt * 8 + 2 * t;
+      if (ra_ok) {
+        if (c < s) out[(size_t)c * ld + ra] = acc[nt][0];
+        if (c + 1 < s) out[(size_t)(c + 1) * ld + ra] = acc[nt][1];
+      }
+      if (rb_ok) {
+        if (c < s) out[(size_t)c * ld + rb] = acc[nt][2];
+        if (c + 1 < s) out[(size_t)(c + 1) * ld + rb] = acc[nt][3];
+      }
+    }
+  }
+  if (want_norm) {
+    double dn = nrm;
+    for (int o = 16; o > 0; o >>= 1) dn += __shfl_xor_sync(0xffffffffu, dn, o);
+    if (lane == 0) red[warp] = dn;
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(&a.st[it.x].normA2, red[0] + red[1] + red[2] + red[3]);
+  }
+}
+
+// Gaussian table for one sample round, rounded to BF16 (the rounded values are
+// the test matrix)
+__global__ void k_omega(float* om, int rows, int bs, uint32_t seed, int round) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)rows * bs;
+       e += (long long)gridDim.x * blockDim.x) {
+    int j = (int)(e / bs), c = (int)(e % bs);
+    float x = gauss_at(seed, 0x51ed270bu + round, (uint32_t)j, (uint32_t)c);
+    om[e] = __uint_as_float(pack_bf16(x, 0.f) << 16);
   }
 }
 
@@ -442,6 +610,241 @@ __global__ void __launch_bounds__(kOrthThreads) k_orth(OrthArgs<W> a) {
 }
 
 // ---------------------------------------------------------------------------
+// truncation: A ~ Q B^T with B = A^T Q; eig(B^T B) = W diag(lambda) W^T gives
+// the singular values of A's approximation, sqrt(lambda), and
+// A ~ (Q W_r)(B W_r)^T with the smallest r whose discarded sum of lambda fits
+// the tolerance left after the sampling residual.  Columns come out in
+// decreasing singular value, U = Q W_r orthonormal, |V_j| = sigma_j.
+// ---------------------------------------------------------------------------
+constexpr int kGramThreads = 256;
+
+// G = B^T B (k x k, FP64) into global memory at goff, 8x8 register tiles
+template <typename W>
+__global__ void __launch_bounds__(kGramThreads) k_gram_big(const Prob* probs, const ProbState* st, const W* ws,
+                                                           const long long* goff, double* G) {
+  __shared__ double Bs[16][kMaxCols + 1];
+  const int p = blockIdx.x;
+  const int k = st[p].k;
+  if (k <= 1) return;
+  const Prob P = probs[p];
+  const W* B = ws + P.boff;
+  const int nt = (k + 7) / 8;
+  const int t = threadIdx.x;
+  const int ti = t / 16, tj = t % 16;  // tile (ti, tj) of up to 16 x 16 tiles
+  const bool active = ti < nt && tj < nt && ti <= tj;
+  double acc[8][8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+  for (int i0 = 0; i0 < P.n; i0 += 16) {
+    for (int e = t; e < 16 * k; e += kGramThreads) {
+      int ii = e % 16, j = e / 16;
+      Bs[ii][j] = (i0 + ii < P.n) ? (double)B[(size_t)j * P.n + i0 + ii] : 0.0;
+    }
+    __syncthreads();
+    if (active) {
+      for (int ii = 0; ii < 16; ++ii) {
+        double x[8], y[8];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+          int ja = ti * 8 + a, jb = tj * 8 + a;
+          x[a] = ja < k ? Bs[ii][ja] : 0.0;
+          y[a] = jb < k ? Bs[ii][jb] : 0.0;
+        }
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+          for (int b = 0; b < 8; ++b) acc[a][b] = fma(x[a], y[b], acc[a][b]);
+      }
+    }
+    __syncthreads();
+  }
+  if (active) {
+    double* g = G + goff[p];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        int ja = ti * 8 + a, jb = tj * 8 + b;
+        if (ja < k && jb < k) {
+          g[ja * k + jb] = acc[a][b];
+          g[jb * k + ja] = acc[a][b];
+        }
+      }
+  }
+}
+
+// Parallel cyclic Jacobi on G (k x k) in shared memory; the rotations are
+// accumulated into Wm (FP32).  Writes the truncated rank to st[p].r and the
+// leading r eigenvectors (columns in decreasing eigenvalue) to Wr (k x r, at
+// the same offset as G).
+__global__ void __launch_bounds__(kGramThreads) k_jacobi(const Prob* probs, ProbState* st, const long long* goff,
+                                                         const double* Gin, float* Wr, double tol2) {
+  extern __shared__ __align__(16) unsigned char jsm[];
+  const int p = blockIdx.x;
+  ProbState S = st[p];
+  const int k = S.k;
+  const int t = threadIdx.x;
+  if (k <= 1) {
+    if (t == 0) {
+      st[p].r = k;
+      if (k == 1) Wr[goff[p]] = 1.f;
+    }
+    return;
+  }
+  const int kp = (k + 1) & ~1;  // even size: an odd k gets a zero row and column
+  double* G = reinterpret_cast<double*>(jsm);              // [kp][kp]
+  float* Wm = reinterpret_cast<float*>(G + kp * kp);        // [kp][kp]
+  double* cs = reinterpret_cast<double*>(Wm + kp * kp);     // [kp/2][2]
+  int* pr = reinterpret_cast<int*>(cs + kp);                // [kp] tournament positions
+  int* order = pr + kp;                                     // [kp]
+  __shared__ double off_sh;
+  const double* g = Gin + goff[p];
+  for (int e = t; e < kp * kp; e += kGramThreads) {
+    int a = e / kp, b = e % kp;
+    G[e] = (a < k && b < k) ? g[a * k + b] : 0.0;
+    Wm[e] = a == b ? 1.f : 0.f;
+  }
+  for (int i = t; i < kp; i += kGramThreads) pr[i] = i;
+  __syncthreads();
+  double scale = 0;
+  for (int i = 0; i < k; ++i) scale += G[i * kp + i];
+  const int npairs = kp / 2;
+  for (int sweep = 0; sweep < 12; ++sweep) {
+    if (t == 0) off_sh = 0;
+    __syncthreads();
+    for (int step = 0; step < kp - 1; ++step) {
+      // pair i: (pr[i], pr[kp-1-i]); angles
+      for (int i = t; i < npairs; i += kGramThreads) {
+        int a = pr[i], b = pr[kp - 1 - i];
+        int pp = min(a, b), qq = max(a, b);
+        double apq = G[pp * kp + qq];
+        double c = 1, s = 0;
+        if (fabs(apq) > 1e-300 && fabs(apq) > 1e-18 * scale) {
+          double th = (G[qq * kp + qq] - G[pp * kp + pp]) / (2 * apq);
+          double tt = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+          c = 1.0 / sqrt(tt * tt + 1.0);
+          s = tt * c;
+          atomicAdd(&off_sh, apq * apq);
+        }
+        cs[2 * i] = c;
+        cs[2 * i + 1] = s;
+      }
+      __syncthreads();
+      // rows
+      for (int e = t; e < npairs * kp; e += kGramThreads) {
+        int i = e / kp, j = e % kp;
+        int a = pr[i], b = pr[kp - 1 - i];
+        int pp = min(a, b), qq = max(a, b);
+        double c = cs[2 * i], s = cs[2 * i + 1];
+        double gp = G[pp * kp + j], gq = G[qq * kp + j];
+        G[pp * kp + j] = c * gp - s * gq;
+        G[qq * kp + j] = s * gp + c * gq;
+      }
+      __syncthreads();
+      // columns, and the accumulated rotation
+      for (int e = t; e < npairs * kp; e += kGramThreads) {
+        int i = e / kp, j = e % kp;
+        int a = pr[i], b = pr[kp - 1 - i];
+        int pp = min(a, b), qq = max(a, b);
+        double c = cs[2 * i], s = cs[2 * i + 1];
+        double gp = G[j * kp + pp], gq = G[j * kp + qq];
+        G[j * kp + pp] = c * gp - s * gq;
+        G[j * kp + qq] = s * gp + c * gq;
+        float wp = Wm[j * kp + pp], wq = Wm[j * kp + qq];
+        Wm[j * kp + pp] = (float)(c * wp - s * wq);
+        Wm[j * kp + qq] = (float)(s * wp + c * wq);
+      }
+      __syncthreads();
+      // next tournament round: keep position 0, rotate the rest
+      if (t == 0) {
+        int last = pr[kp - 1];
+        for (int i = kp - 1; i > 1; --i) pr[i] = pr[i - 1];
+        pr[1] = last;
+      }
+      __syncthreads();
+    }
+    if (off_sh <= 1e-26 * scale * scale) break;
+    __syncthreads();
+  }
+  // order by decreasing eigenvalue (rank by counting), then the rank
+  for (int i = t; i < k; i += kGramThreads) {
+    double li = G[i * kp + i];
+    int rk = 0;
+    for (int j = 0; j < k; ++j) {
+      double lj = G[j * kp + j];
+      rk += (lj > li) || (lj == li && j < i);
+    }
+    order[rk] = i;
+  }
+  __syncthreads();
+  __shared__ int r_sh;
+  if (t == 0) {
+    // discard the smallest eigenvalues while their sum fits the budget
+    double budget = tol2 * S.normA2 - S.est;
+    double tail = 0;
+    int r = k;
+    if (S.converged && budget > 0) {
+      while (r > 1) {
+        double l = fmax(G[order[r - 1] * kp + order[r - 1]], 0.0);
+        if (tail + l > budget) break;
+        tail += l;
+        --r;
+      }
+    }
+    r_sh = r;
+    st[p].r = r;
+  }
+  __syncthreads();
+  const int r = r_sh;
+  float* w = Wr + goff[p];
+  for (int e = t; e < k * r; e += kGramThreads) {
+    int a = e % k, c = e / k;
+    w[c * k + a] = Wm[a * kp + order[c]];  // column c: eigenvector order[c]
+  }
+}
+
+// U = Q W_r (m x r), V = B W_r (n x r), FP32
+template <typename W>
+__global__ void k_pack_trunc(const Prob* probs, const ProbState* st, const W* ws, const long long* goff,
+                             const float* Wr, const long long* dst_u, const long long* dst_v, float* dst) {
+  const int p = blockIdx.x;
+  const int k = st[p].k, r = st[p].r;
+  if (dst_u[p] < 0 || r <= 0) return;
+  const Prob P = probs[p];
+  const float* w = Wr + goff[p];
+  __shared__ float ws_sh[kMaxCols * 32];
+  const int rc = min(r, 32);
+  for (int c0 = 0; c0 < r; c0 += 32) {
+    const int nc = min(32, r - c0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < k * nc; e += blockDim.x) ws_sh[e] = w[(size_t)(c0 + e / k) * k + e % k];
+    __syncthreads();
+    for (int side = 0; side < 2; ++side) {
+      const int rows = side ? P.n : P.m;
+      const W* src = ws + (side ? P.boff : P.qoff);
+      float* out = dst + (side ? dst_v[p] : dst_u[p]);
+      for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+        float acc[32];
+        for (int c = 0; c < nc; ++c) acc[c] = 0.f;
+        for (int a = 0; a < k; ++a) {
+          float x = (float)src[(size_t)a * rows + i];
+          for (int c = 0; c < nc; ++c) acc[c] = fmaf(x, ws_sh[c * k + a], acc[c]);
+        }
+        for (int c = 0; c < nc; ++c) out[(size_t)(c0 + c) * rows + i] = acc[c];
+      }
+    }
+  }
+  (void)rc;
+}
+
+size_t jacobi_smem(int kmax) {
+  int kp = (kmax + 1) & ~1;
+  return sizeof(double) * kp * kp + sizeof(float) * kp * kp + sizeof(double) * kp + sizeof(int) * 2 * kp + 64;
+}
+
+// ---------------------------------------------------------------------------
 // packing and dense blocks
 // ---------------------------------------------------------------------------
 struct PackItem {
@@ -578,7 +981,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
 
   // per-problem results that survive the batch: the factor location
   std::vector<const float*> fu(nprob, nullptr), fv(nprob, nullptr);
-  std::vector<const float*> fd(nprob, nullptr);
+  std::vector<const float*> fd(nprob, nullptr), fdt(nprob, nullptr);
 
   // Sketches, bases and projections run in FP64 when the tolerance is below
   // what FP32 sums over a block can resolve (~u*sqrt(m) relative), else FP32.
@@ -650,12 +1053,40 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       oa.ws = ws.p;
       oa.bs = bs;
       oa.thresh2 = thresh2;
+      // FP32 working precision: sketch products on the tensor cores
+      constexpr bool kTensor = std::is_same<W, float>::value;
+      KmmTcArgs kt;
+      DevBuf<float> omega;
+      if constexpr (kTensor) {
+        int max_n = 1;
+        for (const Prob& P : bp) max_n = std::max(max_n, P.n);
+        if ((st = omega.alloc_async((size_t)max_n * bs, stream))) return st;
+        kt.probs = dprobs.p;
+        kt.st = dst.p;
+        kt.pts = t->pts_tree_f.p;
+        kt.npts = t->n;
+        kt.d = t->d;
+        kt.kp = h->kp;
+        kt.bs = bs;
+        kt.omega = omega.p;
+        kt.ws = reinterpret_cast<float*>(ws.p);
+        kt.omega_rows = max_n;
+      }
       const int max_rounds = kMaxCols / bs + 2;
       for (int round = 0; round < max_rounds; ++round) {
-        ka.mode = 0;
-        ka.round = round;
-        ka.items = drows.p;
-        k_kmm<W><<<(unsigned)items_rows.size(), kKmmThreads, kmm_smem<W>(), stream>>>(ka);
+        if constexpr (kTensor) {
+          k_omega<<<592, 256, 0, stream>>>(omega.p, kt.omega_rows, bs, ka.seed, round);
+          HM_LAUNCH_CHECK();
+          kt.mode = 0;
+          kt.round = round;
+          kt.items = drows.p;
+          k_kmm_tc<<<(unsigned)items_rows.size(), 128, 0, stream>>>(kt);
+        } else {
+          ka.mode = 0;
+          ka.round = round;
+          ka.items = drows.p;
+          k_kmm<W><<<(unsigned)items_rows.size(), kKmmThreads, kmm_smem<W>(), stream>>>(ka);
+        }
         HM_LAUNCH_CHECK();
         oa.round = round;
         k_orth<W><<<nb, kOrthThreads, orth_smem<W>(), stream>>>(oa);
@@ -667,13 +1098,47 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
         if (!any) break;
       }
       // B = A^T Q
-      ka.mode = 1;
-      ka.items = dcols.p;
-      k_kmm<W><<<(unsigned)items_cols.size(), kKmmThreads, kmm_smem<W>(), stream>>>(ka);
+      if constexpr (kTensor) {
+        kt.mode = 1;
+        kt.items = dcols.p;
+        k_kmm_tc<<<(unsigned)items_cols.size(), 128, 0, stream>>>(kt);
+      } else {
+        ka.mode = 1;
+        ka.items = dcols.p;
+        k_kmm<W><<<(unsigned)items_cols.size(), kKmmThreads, kmm_smem<W>(), stream>>>(ka);
+      }
       HM_LAUNCH_CHECK();
 
+      // ---- truncation: Gram of B, Jacobi eigen, truncated rank -------------
+      HM_CUDA(cudaMemcpyAsync(hst.data(), dst.p, sizeof(ProbState) * nb, cudaMemcpyDeviceToHost, stream));
+      HM_CUDA(cudaStreamSynchronize(stream));
+      std::vector<long long> goff(nb);
+      size_t gtot = 0;
+      int kbig = 2;
+      for (int i = 0; i < nb; ++i) {
+        goff[i] = (long long)gtot;
+        gtot += (size_t)hst[i].k * hst[i].k;
+        kbig = std::max(kbig, hst[i].k);
+      }
+      DevBuf<long long> dgoff;
+      DevBuf<double> Gbuf;
+      DevBuf<float> Wr;
+      if ((st = dgoff.alloc_async(nb, stream)) || (st = Gbuf.alloc_async(std::max<size_t>(gtot, 1), stream)) ||
+          (st = Wr.alloc_async(std::max<size_t>(gtot, 1), stream)))
+        return st;
+      HM_CUDA(cudaMemcpyAsync(dgoff.p, goff.data(), sizeof(long long) * nb, cudaMemcpyHostToDevice, stream));
+      k_gram_big<W><<<nb, kGramThreads, 0, stream>>>(dprobs.p, dst.p, ws.p, dgoff.p, Gbuf.p);
+      HM_LAUNCH_CHECK();
+      HM_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)jacobi_smem(kMaxCols)));
+      k_jacobi<<<nb, kGramThreads, jacobi_smem(kbig), stream>>>(dprobs.p, dst.p, dgoff.p, Gbuf.p, Wr.p,
+                                                                 0.45 * opt.tol * opt.tol);
+      HM_LAUNCH_CHECK();
+      HM_CUDA(cudaMemcpyAsync(hst.data(), dst.p, sizeof(ProbState) * nb, cudaMemcpyDeviceToHost, stream));
+      HM_CUDA(cudaStreamSynchronize(stream));
+
       // ---- results: low rank where converged, dense otherwise ---------------
-      std::vector<PackItem> packs;
+      std::vector<long long> du(nb, -1), dv(nb, -1);
       std::vector<DenseItem> dens;
       size_t chunk_floats = 0;
       for (int i = 0; i < nb; ++i) {
@@ -687,20 +1152,15 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
         const bool small = (size_t)P.m * P.n <= 2 * (size_t)(P.m + P.n) * (size_t)std::max(S.k, 1);
         if (!(S.converged || S.active) && !(P.level == depth || small)) ++unconverged;
         if (S.converged || S.active || !(P.level == depth || small)) {
-          PackItem pi;
-          pi.src_q = P.qoff;
-          pi.src_b = P.boff;
-          pi.m = P.m;
-          pi.n = P.n;
-          pi.k = S.k;
-          pi.dst_u = (long long)chunk_floats;
-          chunk_floats += (size_t)P.m * S.k;
-          pi.dst_v = (long long)chunk_floats;
-          chunk_floats += (size_t)P.n * S.k;
-          packs.push_back(pi);
-          rank[gi] = S.k;
+          du[i] = (long long)chunk_floats;
+          chunk_floats += (size_t)P.m * S.r;
+          dv[i] = (long long)chunk_floats;
+          chunk_floats += (size_t)P.n * S.r;
+          rank[gi] = S.r;
           conv[gi] = 1;
         } else {
+          // the block and its mirror, each column-major, so every dense read in
+          // the matvec is coalesced
           DenseItem di;
           di.r0 = P.r0;
           di.m = P.m;
@@ -709,22 +1169,28 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
           di.off = (long long)chunk_floats;
           chunk_floats += (size_t)P.m * P.n;
           dens.push_back(di);
+          DenseItem dt;
+          dt.r0 = P.c0;
+          dt.m = P.n;
+          dt.c0 = P.r0;
+          dt.n = P.m;
+          dt.off = (long long)chunk_floats;
+          chunk_floats += (size_t)P.m * P.n;
+          dens.push_back(dt);
           rank[gi] = -1;
         }
       }
       DevBuf<float> chunk;
       if ((st = chunk.alloc(std::max<size_t>(chunk_floats, 1)))) return st;
-      DevBuf<PackItem> dpk;
+      DevBuf<long long> ddu, ddv;
       DevBuf<DenseItem> ddi;
-      if (!packs.empty()) {
-        if ((st = dpk.alloc(packs.size()))) return st;
-        HM_CUDA(cudaMemcpyAsync(dpk.p, packs.data(), sizeof(PackItem) * packs.size(), cudaMemcpyHostToDevice,
-                                stream));
-        k_pack<W><<<(unsigned)packs.size(), 256, 0, stream>>>(dpk.p, (int)packs.size(), ws.p, chunk.p);
-        HM_LAUNCH_CHECK();
-      }
+      if ((st = ddu.alloc_async(nb, stream)) || (st = ddv.alloc_async(nb, stream))) return st;
+      HM_CUDA(cudaMemcpyAsync(ddu.p, du.data(), sizeof(long long) * nb, cudaMemcpyHostToDevice, stream));
+      HM_CUDA(cudaMemcpyAsync(ddv.p, dv.data(), sizeof(long long) * nb, cudaMemcpyHostToDevice, stream));
+      k_pack_trunc<W><<<nb, 256, 0, stream>>>(dprobs.p, dst.p, ws.p, dgoff.p, Wr.p, ddu.p, ddv.p, chunk.p);
+      HM_LAUNCH_CHECK();
       if (!dens.empty()) {
-        if ((st = ddi.alloc(dens.size()))) return st;
+        if ((st = ddi.alloc_async(dens.size(), stream))) return st;
         HM_CUDA(cudaMemcpyAsync(ddi.p, dens.data(), sizeof(DenseItem) * dens.size(), cudaMemcpyHostToDevice,
                                 stream));
         k_dense_gen<<<(unsigned)dens.size(), 256, 0, stream>>>(ddi.p, t->pts_tree_f.p, t->n, t->d, h->kp,
@@ -736,8 +1202,8 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       for (int i = 0; i < nb; ++i) {
         long long gi = pstart + i;
         if (rank[gi] >= 0) {
-          fu[gi] = chunk.p + packs[pk].dst_u;
-          fv[gi] = chunk.p + packs[pk].dst_v;
+          fu[gi] = chunk.p + du[i];
+          fv[gi] = chunk.p + dv[i];
           ++pk;
           lr_count += 2;
           rank_sum += 2 * (long long)rank[gi];
@@ -745,9 +1211,10 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
           factor_bytes += 4ll * (bp[i].m + bp[i].n) * rank[gi];
         } else {
           fd[gi] = chunk.p + dens[dk].off;
-          ++dk;
+          fdt[gi] = chunk.p + dens[dk + 1].off;
+          dk += 2;
           dense_count += 2;
-          dense_bytes += 4ll * bp[i].m * bp[i].n;
+          dense_bytes += 8ll * bp[i].m * bp[i].n;
         }
       }
       h->storage.push_back(std::move(chunk));
@@ -821,7 +1288,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
     } else {
       DenseBlock db{P.r0, P.m, P.c0, P.n, 0, fd[i]};
       h->h_dense.push_back(db);
-      DenseBlock dt{P.c0, P.n, P.r0, P.m, 1, fd[i]};
+      DenseBlock dt{P.c0, P.n, P.r0, P.m, 0, fdt[i]};
       h->h_dense.push_back(dt);
     }
   }

@@ -19,23 +19,39 @@ struct LRBlock {
 
 struct DenseBlock {
   int r0, m, c0, n;
-  int trans;       // 0: D is m x n (ld m); 1: D is stored n x m (ld n), use D^T
+  int trans;       // always 0: D is m x n, column-major (ld m); mirrors are stored transposed
   const float* D;
 };
 
+struct P1Item {
+  int block;       // index into the low-rank block list
+  int chunk;       // 512-row chunk of the block's V
+  long long part;  // -1: the block has one chunk and stores T_b; else offset of this chunk's partial
+};
+
+struct MultiItem {  // a block whose projection is the sum of several chunk partials
+  long long toff;   // T_b
+  long long poff;   // first partial
+  int kpad, nch;
+};
+
 struct MatvecPlan {
-  // low-rank blocks, and for phase 2 the CSR of low-rank blocks per leaf row:
-  // every block whose row cluster contains the leaf
-  DevBuf<LRBlock> lr;
-  DevBuf<int> p1_items;      // phase 1 work items: block index << 8 | chunk (see hm_matvec.cu)
+  DevBuf<LRBlock> lr;        // low-rank blocks, both orientations
+  DevBuf<P1Item> p1;         // phase 1 work items (one warp each)
   int num_p1 = 0;
+  DevBuf<MultiItem> multi;  // projections summed over several chunk partials
+  int num_multi = 0;
+  long long part_floats = 0;  // partials, stored after the projections in T
+  DevBuf<int2> groups;       // phase 2 work items: (leaf, first row of a 32-row group)
+  int num_groups = 0;
   DevBuf<int> leaf_ptr;      // 2^depth + 1
   DevBuf<int> leaf_blk;      // low-rank blocks covering each leaf row
   DevBuf<DenseBlock> dense;  // dense blocks
   DevBuf<int> leaf_dptr;     // 2^depth + 1
   DevBuf<int> leaf_dblk;     // dense blocks of each leaf row
-  DevBuf<float> T;           // projections workspace (sum_b k_b * nrhs_cap)
-  long long t_per_rhs = 0;   // sum_b k_b
+  DevBuf<float> T;           // projections: per block 16 x kpad_b, then the chunk partials
+  long long t_floats = 0;    // sum_b 16 * kpad_b
+  long long t_per_rhs = 0;   // sum_b kpad_b
   int nrhs_cap = 0;
   int num_leaves = 0;
   int maxleaf = 1;

@@ -5,21 +5,25 @@
 // a grouped GEMM T = V^T X and a grouped GEMM Y += U T, with a host round trip
 // per level (src/cutlassHMatrixXVector.cu:50-398), for weak admissibility only.
 //
-// Here the product is two launches for any admissibility:
-//   phase 1 (projection): T_b = V_b^T X[cols(b)] for every low-rank block b,
-//     one work item per (block, 1024-row chunk of V_b), reduced in shared
-//     memory and added into T_b;
-//   phase 2 (expansion): one CTA per leaf row cluster accumulates, in
-//     registers, U_b[rows of the leaf] T_b over every low-rank block whose row
-//     cluster contains the leaf (all levels) plus the leaf's dense blocks times
-//     X, and writes its rows of Y once (no atomics on Y).
-// Both launches are stream ordered and allocation free; X/Y in the points'
-// original order are gathered / scattered through the tree permutation.
+// Here the product is two launches for any admissibility.  Both are warp-level
+// tensor-core kernels whose operands are loaded straight from HBM in MMA
+// fragment order (no shared memory, no block-wide barriers); 16 right-hand
+// sides form the MMA's M dimension:
+//   phase 1 (projection) T_b^T = X[cols(b)]^T V_b: one warp per (block, chunk
+//     of <= 256 rows of V_b); the MMA accumulates over the rows; blocks with
+//     several chunks write per-chunk partials that a small kernel sums in
+//     chunk order (bitwise reproducible);
+//   phase 2 (expansion) Y^T = sum_b T_b^T U_b^T + sum_D X^T D^T: one warp per
+//     32 rows of a leaf, over every low-rank block covering the leaf (all
+//     levels) and the leaf's dense blocks; Y is written once, no atomics.
+// FP32 factors use three TF32 passes (hi/lo split of both operands), which
+// reproduces FP32 products.
 #include <algorithm>
 #include <mutex>
 #include <numeric>
 
 #include "hm_hmatrix.h"
+#include "hm_mma.cuh"
 #include "hm_structure.h"
 
 // Scratch of the allocation-free product (hm_hmatvec_noalloc): 4 Mi floats
@@ -32,138 +36,218 @@ static __device__ __align__(256) float hm_noalloc_scratch[size_t(4) << 20];
 namespace hm {
 namespace {
 
-constexpr int kP1Rows = 1024;
-constexpr int kThreads = 256;
+constexpr int kP1Rows = 256;
+constexpr int kWarpsPerCta = 4;
 constexpr int kMaxK = 128;
-constexpr int kMaxOut = 16;  // outputs per thread
+constexpr int kMaxTiles = kMaxK / 8;
 
-__global__ void __launch_bounds__(kThreads) k_mv_project(const int2* items, const LRBlock* lr,
-                                                         const float* X, int ldx, int nrhs, float* T) {
-  extern __shared__ __align__(16) float sm[];
-  float* Vs = sm;                 // [kMaxK][33]
-  float* Xs = Vs + kMaxK * 33;    // [32][33]
-  const int2 it = items[blockIdx.x];
-  const LRBlock B = lr[it.x];
-  const int k = B.k;
-  const int i_lo = it.y * kP1Rows;
-  const int i_hi = min(B.n, i_lo + kP1Rows);
-  const int nout = k * nrhs;
-  const int t = threadIdx.x;
-  float acc[kMaxOut];
+// ---------------------------------------------------------------------------
+// phase 1
+// ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// phase 1: T_b^T (16 x kpad) = X^T V_b over a chunk of rows.  NT: tile count
+// the code is compiled for (>= the block's), U: k-steps (8 rows each) whose
+// loads are issued together before their MMAs.
+// ---------------------------------------------------------------------------
+template <int NT, int U>
+__device__ __forceinline__ void p1_item(const LRBlock& B, int i_lo, int i_hi, const float* __restrict__ X, int ldx,
+                                        int nr, float* out, int g, int t) {
+  const int k = B.k, kpad = (k + 7) & ~7, ntiles = kpad >> 3;
+  const float* __restrict__ V = B.V;
+  const float* __restrict__ xg = X + (size_t)g * ldx + B.c0;
+  const float* __restrict__ xg8 = X + (size_t)(g + 8) * ldx + B.c0;
+  const bool g_ok = g < nr, g8_ok = g + 8 < nr;
+  float acc[NT][4];
 #pragma unroll
-  for (int x = 0; x < kMaxOut; ++x) acc[x] = 0.f;
-  for (int i0 = i_lo; i0 < i_hi; i0 += 32) {
-    for (int e = t; e < 32 * k; e += kThreads) {
-      int ii = e & 31, j = e >> 5;
-      int i = i0 + ii;
-      Vs[j * 33 + ii] = i < i_hi ? B.V[(size_t)j * B.n + i] : 0.f;
-    }
-    for (int e = t; e < 32 * nrhs; e += kThreads) {
-      int ii = e & 31, c = e >> 5;
-      int i = i0 + ii;
-      Xs[c * 33 + ii] = i < i_hi ? X[(size_t)c * ldx + B.c0 + i] : 0.f;
-    }
-    __syncthreads();
+  for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+  for (int i0 = i_lo; i0 < i_hi; i0 += 8 * U) {
+    float xa[U][4], vb[U][NT][2];
 #pragma unroll
-    for (int x = 0; x < kMaxOut; ++x) {
-      int o = t + x * kThreads;
-      if (o < nout) {
-        int j = o / nrhs, c = o % nrhs;
-        float s = acc[x];
-#pragma unroll 8
-        for (int ii = 0; ii < 32; ++ii) s = fmaf(Vs[j * 33 + ii], Xs[c * 33 + ii], s);
-        acc[x] = s;
+    for (int u = 0; u < U; ++u) {
+      const int ra = i0 + 8 * u + t, rb = ra + 4;
+      const bool ra_ok = ra < i_hi, rb_ok = rb < i_hi;
+      xa[u][0] = g_ok && ra_ok ? __ldg(xg + ra) : 0.f;
+      xa[u][1] = g8_ok && ra_ok ? __ldg(xg8 + ra) : 0.f;
+      xa[u][2] = g_ok && rb_ok ? __ldg(xg + rb) : 0.f;
+      xa[u][3] = g8_ok && rb_ok ? __ldg(xg8 + rb) : 0.f;
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) {
+        const int col = nt * 8 + g;
+        const bool c_ok = nt < ntiles && col < k;
+        const float* vc = V + (size_t)col * B.n;
+        vb[u][nt][0] = c_ok && ra_ok ? __ldcs(vc + ra) : 0.f;
+        vb[u][nt][1] = c_ok && rb_ok ? __ldcs(vc + rb) : 0.f;
       }
     }
-    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      uint32_t ah[4], al[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) split_tf32(xa[u][q], ah[q], al[q]);
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) {
+        if (nt < ntiles) {
+          uint32_t bh0, bl0, bh1, bl1;
+          split_tf32(vb[u][nt][0], bh0, bl0);
+          split_tf32(vb[u][nt][1], bh1, bl1);
+          mma_3xtf32(acc[nt], ah, al, bh0, bh1, bl0, bl1);
+        }
+      }
+    }
   }
 #pragma unroll
-  for (int x = 0; x < kMaxOut; ++x) {
-    int o = t + x * kThreads;
-    if (o < nout) atomicAdd(&T[B.toff + o], acc[x]);  // T_b[j * nrhs + c]
+  for (int nt = 0; nt < NT; ++nt) {
+    if (nt < ntiles) {
+      const int j = nt * 8 + 2 * t;
+      *reinterpret_cast<float2*>(out + (size_t)g * kpad + j) = make_float2(acc[nt][0], acc[nt][1]);
+      *reinterpret_cast<float2*>(out + (size_t)(g + 8) * kpad + j) = make_float2(acc[nt][2], acc[nt][3]);
+    }
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_mv_expand(const int* leaf_off, const int* leaf_ptr,
-                                                        const int* leaf_blk, const LRBlock* lr,
-                                                        const int* leaf_dptr, const int* leaf_dblk,
-                                                        const DenseBlock* dense, const float* T,
-                                                        const float* X, int ldx, float* Y, int ldy,
-                                                        int nrhs) {
-  extern __shared__ __align__(16) float sm[];
-  const int leaf = blockIdx.x;
-  const int r_lo = leaf_off[leaf], rows = leaf_off[leaf + 1] - r_lo;
-  if (rows <= 0) return;
-  float* Us = sm;                     // [kMaxK][rows]
-  float* Ts = Us + kMaxK * rows;      // [kMaxK][nrhs]
-  float* Ds = Ts + kMaxK * nrhs;      // [32][rows]
-  float* Xs = Ds + 32 * rows;         // [32][nrhs]
-  const int t = threadIdx.x;
-  const int nout = rows * nrhs;
-  float acc[kMaxOut];
-#pragma unroll
-  for (int x = 0; x < kMaxOut; ++x) acc[x] = 0.f;
+__global__ void __launch_bounds__(32 * kWarpsPerCta) k_p1(const P1Item* items, int nitems, const LRBlock* lr,
+                                                          const float* __restrict__ X, int ldx, int nr,
+                                                          float* __restrict__ T, float* __restrict__ Tpart) {
+  const int w = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
+  if (w >= nitems) return;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const P1Item it = items[w];
+  const LRBlock B = lr[it.block];
+  const int i_lo = it.chunk * kP1Rows;
+  const int i_hi = min(B.n, i_lo + kP1Rows);
+  float* out = it.part >= 0 ? Tpart + it.part : T + B.toff;  // [16][kpad]
+  if (B.k <= 8)
+    p1_item<1, 8>(B, i_lo, i_hi, X, ldx, nr, out, g, t);
+  else if (B.k <= 16)
+    p1_item<2, 4>(B, i_lo, i_hi, X, ldx, nr, out, g, t);
+  else if (B.k <= 32)
+    p1_item<4, 4>(B, i_lo, i_hi, X, ldx, nr, out, g, t);
+  else
+    p1_item<kMaxTiles, 1>(B, i_lo, i_hi, X, ldx, nr, out, g, t);
+}
 
-  for (int q = leaf_ptr[leaf]; q < leaf_ptr[leaf + 1]; ++q) {
-    const LRBlock B = lr[leaf_blk[q]];
-    const int k = B.k;
-    const int off = r_lo - B.r0;
-    for (int e = t; e < k * rows; e += kThreads) {
-      int i = e % rows, j = e / rows;
-      Us[j * rows + i] = B.U[(size_t)j * B.m + off + i];
+// projections of blocks split into several chunks: sum the chunk partials in
+// chunk order (deterministic)
+__global__ void k_reduce_multi(const MultiItem* mi, int n, const float* __restrict__ Tpart, float* __restrict__ T) {
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const MultiItem M = mi[b];
+    const int len = 16 * M.kpad;
+    for (int e = threadIdx.x; e < len; e += blockDim.x) {
+      float sacc = 0.f;
+      for (int c = 0; c < M.nch; ++c) sacc += Tpart[M.poff + (long long)c * len + e];
+      T[M.toff + e] = sacc;
     }
-    for (int e = t; e < k * nrhs; e += kThreads) Ts[e] = T[B.toff + e];
-    __syncthreads();
-#pragma unroll
-    for (int x = 0; x < kMaxOut; ++x) {
-      int o = t + x * kThreads;
-      if (o < nout) {
-        int i = o % rows, c = o / rows;
-        float s = acc[x];
-        for (int j = 0; j < k; ++j) s = fmaf(Us[j * rows + i], Ts[j * nrhs + c], s);
-        acc[x] = s;
-      }
-    }
-    __syncthreads();
   }
-  for (int q = leaf_dptr[leaf]; q < leaf_dptr[leaf + 1]; ++q) {
-    const DenseBlock D = dense[leaf_dblk[q]];
-    const int doff = r_lo - D.r0;  // a dense block may span several leaves
-    for (int j0 = 0; j0 < D.n; j0 += 32) {
-      for (int e = t; e < 32 * rows; e += kThreads) {
-        int i = e % rows, jj = e / rows;
-        int j = j0 + jj;
-        float v = 0.f;
-        if (j < D.n)
-          v = D.trans ? D.D[(size_t)(doff + i) * D.n + j] : D.D[(size_t)j * D.m + doff + i];
-        Ds[jj * rows + i] = v;
-      }
-      for (int e = t; e < 32 * nrhs; e += kThreads) {
-        int jj = e & 31, c = e >> 5;
-        int j = j0 + jj;
-        Xs[jj * nrhs + c] = j < D.n ? X[(size_t)c * ldx + D.c0 + j] : 0.f;
-      }
-      __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// phase 2: Y^T (16 x 32 rows) = sum_b T_b^T U_b^T + sum_D X^T D^T
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(32 * kWarpsPerCta) k_p2(const int2* groups, int ngroups, const int* leaf_off,
+                                                          const int* leaf_ptr, const int* leaf_blk,
+                                                          const LRBlock* lr, const int* leaf_dptr,
+                                                          const int* leaf_dblk, const DenseBlock* dense,
+                                                          const float* __restrict__ T,
+                                                          const float* __restrict__ X, int ldx, int nr,
+                                                          float* __restrict__ Y, int ldy) {
+  const int w = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
+  if (w >= ngroups) return;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int2 gr = groups[w];  // (leaf, first row of the group within the leaf)
+  const int leaf = gr.x;
+  const int l0 = leaf_off[leaf];
+  const int nrow = min(32, leaf_off[leaf + 1] - l0 - gr.y);
+  const int row0 = l0 + gr.y;  // tree-order index of the group's first row
+  float acc[4][4];
 #pragma unroll
-      for (int x = 0; x < kMaxOut; ++x) {
-        int o = t + x * kThreads;
-        if (o < nout) {
-          int i = o % rows, c = o / rows;
-          float s = acc[x];
-#pragma unroll 8
-          for (int jj = 0; jj < 32; ++jj) s = fmaf(Ds[jj * rows + i], Xs[jj * nrhs + c], s);
-          acc[x] = s;
+  for (int nt = 0; nt < 4; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+  const int q_lo = leaf_ptr[leaf], q_hi = leaf_ptr[leaf + 1];
+  for (int qb = q_lo; qb < q_hi; qb += 32) {
+    // descriptors of up to 32 blocks, one per lane, loaded together
+    const int nq = min(32, q_hi - qb);
+    const float* my_u = nullptr;
+    const float* my_t = nullptr;
+    int my_m = 0, my_k = 0;
+    if (lane < nq) {
+      const LRBlock& Bl = lr[leaf_blk[qb + lane]];
+      my_u = Bl.U + (row0 - Bl.r0);
+      my_t = T + Bl.toff;
+      my_m = Bl.m;
+      my_k = Bl.k;
+    }
+    for (int q = 0; q < nq; ++q) {
+      const float* __restrict__ ub =
+          reinterpret_cast<const float*>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(my_u), q));
+      const float* __restrict__ tb =
+          reinterpret_cast<const float*>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(my_t), q));
+      const int m = __shfl_sync(0xffffffffu, my_m, q);
+      const int k = __shfl_sync(0xffffffffu, my_k, q);
+      const int kpad = (k + 7) & ~7;
+      for (int j0 = 0; j0 < kpad; j0 += 8) {
+        uint32_t ah[4], al[4];
+        split_tf32(__ldg(tb + (size_t)g * kpad + j0 + t), ah[0], al[0]);
+        split_tf32(__ldg(tb + (size_t)(g + 8) * kpad + j0 + t), ah[1], al[1]);
+        split_tf32(__ldg(tb + (size_t)g * kpad + j0 + t + 4), ah[2], al[2]);
+        split_tf32(__ldg(tb + (size_t)(g + 8) * kpad + j0 + t + 4), ah[3], al[3]);
+        const bool c0_ok = j0 + t < k, c1_ok = j0 + t + 4 < k;
+        const float* u0 = ub + (size_t)(j0 + t) * m;
+        const float* u1 = ub + (size_t)(j0 + t + 4) * m;
+        float ubuf[4][2];
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          const int rr = nt * 8 + g;
+          const bool r_ok = rr < nrow;
+          ubuf[nt][0] = c0_ok && r_ok ? __ldcs(u0 + rr) : 0.f;
+          ubuf[nt][1] = c1_ok && r_ok ? __ldcs(u1 + rr) : 0.f;
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          uint32_t bh0, bl0, bh1, bl1;
+          split_tf32(ubuf[nt][0], bh0, bl0);
+          split_tf32(ubuf[nt][1], bh1, bl1);
+          mma_3xtf32(acc[nt], ah, al, bh0, bh1, bl0, bl1);
         }
       }
-      __syncthreads();
     }
   }
+  const float* __restrict__ xg = X + (size_t)g * ldx;
+  const float* __restrict__ xg8 = X + (size_t)(g + 8) * ldx;
+  const bool g_ok = g < nr, g8_ok = g + 8 < nr;
+  for (int q = leaf_dptr[leaf]; q < leaf_dptr[leaf + 1]; ++q) {
+    const DenseBlock D = dense[leaf_dblk[q]];
+    const float* __restrict__ db = D.D + (row0 - D.r0);
+    for (int j0 = 0; j0 < D.n; j0 += 8) {
+      const int ca = j0 + t, cb = j0 + t + 4;
+      const bool ca_ok = ca < D.n, cb_ok = cb < D.n;
+      uint32_t ah[4], al[4];
+      split_tf32(g_ok && ca_ok ? __ldg(xg + D.c0 + ca) : 0.f, ah[0], al[0]);
+      split_tf32(g8_ok && ca_ok ? __ldg(xg8 + D.c0 + ca) : 0.f, ah[1], al[1]);
+      split_tf32(g_ok && cb_ok ? __ldg(xg + D.c0 + cb) : 0.f, ah[2], al[2]);
+      split_tf32(g8_ok && cb_ok ? __ldg(xg8 + D.c0 + cb) : 0.f, ah[3], al[3]);
+      const float* d0 = db + (size_t)ca * D.m;
+      const float* d1 = db + (size_t)cb * D.m;
 #pragma unroll
-  for (int x = 0; x < kMaxOut; ++x) {
-    int o = t + x * kThreads;
-    if (o < nout) {
-      int i = o % rows, c = o / rows;
-      Y[(size_t)c * ldy + r_lo + i] = acc[x];
+      for (int nt = 0; nt < 4; ++nt) {
+        const int rr = nt * 8 + g;
+        const bool r_ok = rr < nrow;
+        uint32_t bh0, bl0, bh1, bl1;
+        split_tf32(ca_ok && r_ok ? __ldcs(d0 + rr) : 0.f, bh0, bl0);
+        split_tf32(cb_ok && r_ok ? __ldcs(d1 + rr) : 0.f, bh1, bl1);
+        mma_3xtf32(acc[nt], ah, al, bh0, bh1, bl0, bl1);
+      }
+    }
+  }
+  // acc[nt]: rows nt*8 + 2t, +1 of right-hand sides g and g + 8
+#pragma unroll
+  for (int nt = 0; nt < 4; ++nt) {
+    const int rr = nt * 8 + 2 * t;
+    if (g_ok) {
+      if (rr < nrow) Y[(size_t)g * ldy + row0 + rr] = acc[nt][0];
+      if (rr + 1 < nrow) Y[(size_t)g * ldy + row0 + rr + 1] = acc[nt][1];
+    }
+    if (g8_ok) {
+      if (rr < nrow) Y[(size_t)(g + 8) * ldy + row0 + rr] = acc[nt][2];
+      if (rr + 1 < nrow) Y[(size_t)(g + 8) * ldy + row0 + rr + 1] = acc[nt][3];
     }
   }
 }
@@ -186,8 +270,28 @@ __global__ void k_scatter_rows(const float* Yp, const int* perm, int n, int nrhs
   }
 }
 
-size_t expand_smem(int rows, int nrhs) {
-  return sizeof(float) * ((size_t)kMaxK * rows + (size_t)kMaxK * nrhs + 32 * (size_t)rows + 32 * (size_t)nrhs);
+
+// One panel of nr <= 16 right-hand sides (X, Y in tree order); T: projection
+// scratch (16 x kpad per block, then the chunk partials).
+hm_status run_panel(hm_hmatrix h, int nr, const float* X, int ldx, float* Y, int ldy, float* T, cudaStream_t s,
+                    cudaEvent_t e_mid) {
+  MatvecPlan& P = h->plan;
+  float* Tpart = T + P.t_floats;
+  if (P.num_p1 > 0) {
+    k_p1<<<(P.num_p1 + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, s>>>(P.p1.p, P.num_p1, P.lr.p, X,
+                                                                                     ldx, nr, T, Tpart);
+    HM_LAUNCH_CHECK();
+  }
+  if (P.num_multi > 0) {
+    k_reduce_multi<<<std::min(P.num_multi, 8192), 128, 0, s>>>(P.multi.p, P.num_multi, Tpart, T);
+    HM_LAUNCH_CHECK();
+  }
+  if (e_mid) HM_CUDA(cudaEventRecord(e_mid, s));
+  k_p2<<<(P.num_groups + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, s>>>(
+      P.groups.p, P.num_groups, h->tree->offsets.p, P.leaf_ptr.p, P.leaf_blk.p, P.lr.p, P.leaf_dptr.p,
+      P.leaf_dblk.p, P.dense.p, T, X, ldx, nr, Y, ldy);
+  HM_LAUNCH_CHECK();
+  return HM_OK;
 }
 
 }  // namespace
@@ -197,47 +301,51 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   const int depth = h->depth;
   const int nleaf = 1 << depth;
   const std::vector<int>& lo = h->tree->h_offsets;
-  int maxleaf = 1;
-  for (int l = 0; l < nleaf; ++l) maxleaf = std::max(maxleaf, lo[l + 1] - lo[l]);
-  // rhs panel: at most kMaxOut outputs per thread in phase 2
-  int panel = std::min(32, (kThreads * kMaxOut) / maxleaf);
-  if (panel < 1) return fail(HM_ERR_UNSUPPORTED, "matvec: leaves too large");
-  nrhs_cap = std::min(nrhs_cap, panel);
+  nrhs_cap = 16;
   P.nrhs_cap = nrhs_cap;
   P.num_leaves = nleaf;
-  // T offsets
   long long tk = 0;
   for (auto& b : h->h_lr) {
-    b.toff = tk * nrhs_cap;
-    tk += b.k;
+    if (b.k > kMaxK) return fail(HM_ERR_UNSUPPORTED, "matvec: rank above 128");
+    b.toff = tk;
+    tk += 16ll * ((b.k + 7) & ~7);  // T_b^T: 16 right-hand sides x padded rank
   }
-  P.t_per_rhs = tk;
-  // phase 1 items
-  std::vector<int2> items;
+  P.t_floats = tk;
+  P.t_per_rhs = tk / 16;
+  // phase 1 items; a block spanning several chunks writes one partial per
+  // chunk, summed in chunk order afterwards
+  std::vector<P1Item> items;
+  std::vector<MultiItem> multi;
+  long long part = 0;
   for (size_t i = 0; i < h->h_lr.size(); ++i) {
     const LRBlock& b = h->h_lr[i];
     if (b.k <= 0) continue;
-    for (int c = 0; c * kP1Rows < b.n; ++c) items.push_back(make_int2((int)i, c));
+    int nch = (b.n + kP1Rows - 1) / kP1Rows;
+    const int kpad = (b.k + 7) & ~7;
+    for (int c = 0; c < nch; ++c)
+      items.push_back(P1Item{(int)i, c, nch == 1 ? -1ll : part + (long long)c * 16 * kpad});
+    if (nch > 1) {
+      multi.push_back(MultiItem{b.toff, part, kpad, nch});
+      part += (long long)nch * 16 * kpad;
+    }
   }
   P.num_p1 = (int)items.size();
-  // leaf lists: a block with row range [r0, r0+m) covers the leaves whose
-  // offsets lie in that range (row clusters are unions of consecutive leaves)
+  P.num_multi = (int)multi.size();
+  P.part_floats = part;
+  // phase 2: leaf lists
   auto leaf_range = [&](int r0, int m, int& a, int& b) {
     a = (int)(std::lower_bound(lo.begin(), lo.end() - 1, r0) - lo.begin());
     b = (int)(std::lower_bound(lo.begin(), lo.end() - 1, r0 + m) - lo.begin());
-    // leaves [a, b) have lo[leaf] in [r0, r0+m); empty leaves at the boundary are harmless
   };
   std::vector<int> cnt(nleaf + 1, 0), dcnt(nleaf + 1, 0);
-  std::vector<std::pair<int, int>> ranges(h->h_lr.size());
+  std::vector<std::pair<int, int>> ranges(h->h_lr.size()), dranges(h->h_dense.size());
   for (size_t i = 0; i < h->h_lr.size(); ++i) {
-    const LRBlock& b = h->h_lr[i];
     int a, e;
-    leaf_range(b.r0, b.m, a, e);
+    leaf_range(h->h_lr[i].r0, h->h_lr[i].m, a, e);
     ranges[i] = {a, e};
-    if (b.k <= 0) continue;
-    for (int l = a; l < e; ++l) cnt[l]++;
+    if (h->h_lr[i].k > 0)
+      for (int l = a; l < e; ++l) cnt[l]++;
   }
-  std::vector<std::pair<int, int>> dranges(h->h_dense.size());
   for (size_t i = 0; i < h->h_dense.size(); ++i) {
     int a, e;
     leaf_range(h->h_dense[i].r0, h->h_dense[i].m, a, e);
@@ -257,35 +365,36 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   }
   for (size_t i = 0; i < h->h_dense.size(); ++i)
     for (int l = dranges[i].first; l < dranges[i].second; ++l) dblk[dfill[l]++] = (int)i;
+  std::vector<int2> groups;
+  for (int l = 0; l < nleaf; ++l)
+    for (int r = 0; r < lo[l + 1] - lo[l]; r += 32) groups.push_back(make_int2(l, r));
+  P.num_groups = (int)groups.size();
 
   HM_TRY(P.lr.alloc(std::max<size_t>(h->h_lr.size(), 1)));
-  HM_TRY(P.p1_items.alloc(2 * std::max<size_t>(items.size(), 1)));
+  HM_TRY(P.p1.alloc(std::max<size_t>(items.size(), 1)));
+  HM_TRY(P.multi.alloc(std::max<size_t>(multi.size(), 1)));
+  HM_TRY(P.groups.alloc(std::max<size_t>(groups.size(), 1)));
   HM_TRY(P.leaf_ptr.alloc(nleaf + 1));
   HM_TRY(P.leaf_blk.alloc(blk.size()));
   HM_TRY(P.dense.alloc(std::max<size_t>(h->h_dense.size(), 1)));
   HM_TRY(P.leaf_dptr.alloc(nleaf + 1));
   HM_TRY(P.leaf_dblk.alloc(dblk.size()));
-  HM_TRY(P.T.alloc(std::max<long long>(tk * nrhs_cap, 1)));
+  HM_TRY(P.T.alloc(std::max<long long>(tk + part, 1)));
   HM_TRY(P.Xp.alloc((size_t)h->n * nrhs_cap));
   HM_TRY(P.Yp.alloc((size_t)h->n * nrhs_cap));
-  if (!h->h_lr.empty())
-    HM_CUDA(cudaMemcpyAsync(P.lr.p, h->h_lr.data(), sizeof(LRBlock) * h->h_lr.size(), cudaMemcpyHostToDevice,
-                            stream));
-  if (!items.empty())
-    HM_CUDA(cudaMemcpyAsync(P.p1_items.p, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice,
-                            stream));
-  HM_CUDA(cudaMemcpyAsync(P.leaf_ptr.p, ptr.data(), 4 * (nleaf + 1), cudaMemcpyHostToDevice, stream));
-  HM_CUDA(cudaMemcpyAsync(P.leaf_blk.p, blk.data(), 4 * blk.size(), cudaMemcpyHostToDevice, stream));
-  if (!h->h_dense.empty())
-    HM_CUDA(cudaMemcpyAsync(P.dense.p, h->h_dense.data(), sizeof(DenseBlock) * h->h_dense.size(),
-                            cudaMemcpyHostToDevice, stream));
-  HM_CUDA(cudaMemcpyAsync(P.leaf_dptr.p, dptr.data(), 4 * (nleaf + 1), cudaMemcpyHostToDevice, stream));
-  HM_CUDA(cudaMemcpyAsync(P.leaf_dblk.p, dblk.data(), 4 * dblk.size(), cudaMemcpyHostToDevice, stream));
-  HM_CUDA(cudaFuncSetAttribute(k_mv_expand, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)expand_smem(maxleaf, nrhs_cap)));
-  HM_CUDA(cudaFuncSetAttribute(k_mv_project, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(sizeof(float) * (kMaxK * 33 + 32 * 33))));
-  P.maxleaf = maxleaf;
+  auto up = [&](void* dst, const void* src, size_t bytes) -> hm_status {
+    if (bytes) HM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+    return HM_OK;
+  };
+  HM_TRY(up(P.lr.p, h->h_lr.data(), sizeof(LRBlock) * h->h_lr.size()));
+  HM_TRY(up(P.p1.p, items.data(), sizeof(P1Item) * items.size()));
+  HM_TRY(up(P.multi.p, multi.data(), sizeof(MultiItem) * multi.size()));
+  HM_TRY(up(P.groups.p, groups.data(), sizeof(int2) * groups.size()));
+  HM_TRY(up(P.leaf_ptr.p, ptr.data(), 4 * ptr.size()));
+  HM_TRY(up(P.leaf_blk.p, blk.data(), 4 * blk.size()));
+  HM_TRY(up(P.dense.p, h->h_dense.data(), sizeof(DenseBlock) * h->h_dense.size()));
+  HM_TRY(up(P.leaf_dptr.p, dptr.data(), 4 * dptr.size()));
+  HM_TRY(up(P.leaf_dblk.p, dblk.data(), 4 * dblk.size()));
   HM_CUDA(cudaStreamSynchronize(stream));
   return HM_OK;
 }
@@ -300,8 +409,8 @@ hm_status hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, int ldx, fl
   // dense blocks are generated from a symmetric kernel), so H^T X = H X
   MatvecPlan& P = h->plan;
   const int n = h->n;
-  for (int c0 = 0; c0 < nrhs; c0 += P.nrhs_cap) {
-    const int nr = std::min(P.nrhs_cap, nrhs - c0);
+  for (int c0 = 0; c0 < nrhs;) {
+    const int nr = std::min(16, nrhs - c0);
     const float* Xin = X + (size_t)c0 * ldx;
     float* Yout = Y + (size_t)c0 * ldy;
     const float* Xt = Xin;
@@ -316,24 +425,12 @@ hm_status hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, int ldx, fl
       Yt = P.Yp.p;
       ldyt = n;
     }
-    if (P.t_per_rhs > 0) {
-      HM_CUDA(cudaMemsetAsync(P.T.p, 0, sizeof(float) * (size_t)P.t_per_rhs * P.nrhs_cap, stream));
-    }
-    if (P.num_p1 > 0) {
-      // T offsets were laid out for nrhs_cap columns; a narrower panel uses the
-      // first nr*k entries of each block's slot
-      k_mv_project<<<P.num_p1, kThreads, sizeof(float) * (kMaxK * 33 + 32 * 33), stream>>>(
-          reinterpret_cast<const int2*>(P.p1_items.p), P.lr.p, Xt, ldxt, nr, P.T.p);
-      HM_LAUNCH_CHECK();
-    }
-    k_mv_expand<<<P.num_leaves, kThreads, expand_smem(P.maxleaf, nr), stream>>>(
-        h->tree->offsets.p, P.leaf_ptr.p, P.leaf_blk.p, P.lr.p, P.leaf_dptr.p, P.leaf_dblk.p, P.dense.p, P.T.p,
-        Xt, ldxt, Yt, ldyt, nr);
-    HM_LAUNCH_CHECK();
+    HM_TRY(run_panel(h, nr, Xt, ldxt, Yt, ldyt, P.T.p, stream, nullptr));
     if (original_order) {
       k_scatter_rows<<<592, 256, 0, stream>>>(P.Yp.p, h->tree->perm.p, n, nr, Yout, ldy);
       HM_LAUNCH_CHECK();
     }
+    c0 += nr;
   }
   return HM_OK;
 }
@@ -353,45 +450,6 @@ void matvec_bytes(hm_hmatrix h, int nrhs, long long* b_project, long long* b_exp
   *b_expand = p2;
 }
 
-}  // namespace hm
-
-extern "C" hm_status hm_hmatvec_profile(hm_hmatrix h, int nrhs, const float* X, int ldx, float* Y, int ldy,
-                                        void* stream, float* ms_project, float* ms_expand,
-                                        long long* bytes_project, long long* bytes_expand) {
-  if (!h) return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: null matrix");
-  if (nrhs < 1 || nrhs > h->plan.nrhs_cap || !X || !Y || ldx < h->n || ldy < h->n)
-    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: bad vector arguments (nrhs <= panel width)");
-  cudaStream_t s = hm::as_stream(stream);
-  hm::MatvecPlan& P = h->plan;
-  cudaEvent_t e[3];
-  for (auto& x : e) HM_CUDA(cudaEventCreate(&x));
-  if (P.t_per_rhs > 0) HM_CUDA(cudaMemsetAsync(P.T.p, 0, sizeof(float) * (size_t)P.t_per_rhs * P.nrhs_cap, s));
-  HM_CUDA(cudaEventRecord(e[0], s));
-  if (P.num_p1 > 0)
-    hm::k_mv_project<<<P.num_p1, hm::kThreads, sizeof(float) * (hm::kMaxK * 33 + 32 * 33), s>>>(
-        reinterpret_cast<const int2*>(P.p1_items.p), P.lr.p, X, ldx, nrhs, P.T.p);
-  HM_LAUNCH_CHECK();
-  HM_CUDA(cudaEventRecord(e[1], s));
-  hm::k_mv_expand<<<P.num_leaves, hm::kThreads, hm::expand_smem(P.maxleaf, nrhs), s>>>(
-      h->tree->offsets.p, P.leaf_ptr.p, P.leaf_blk.p, P.lr.p, P.leaf_dptr.p, P.leaf_dblk.p, P.dense.p, P.T.p, X,
-      ldx, Y, ldy, nrhs);
-  HM_LAUNCH_CHECK();
-  HM_CUDA(cudaEventRecord(e[2], s));
-  HM_CUDA(cudaEventSynchronize(e[2]));
-  float a = 0, b = 0;
-  HM_CUDA(cudaEventElapsedTime(&a, e[0], e[1]));
-  HM_CUDA(cudaEventElapsedTime(&b, e[1], e[2]));
-  for (auto& x : e) cudaEventDestroy(x);
-  if (ms_project) *ms_project = a;
-  if (ms_expand) *ms_expand = b;
-  long long bp = 0, be = 0;
-  hm::matvec_bytes(h, nrhs, &bp, &be);
-  if (bytes_project) *bytes_project = bp;
-  if (bytes_expand) *bytes_expand = be;
-  return HM_OK;
-}
-
-namespace hm {
 namespace {
 
 constexpr size_t kNoallocScratchFloats = size_t(4) << 20;
@@ -428,30 +486,21 @@ extern "C" hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, 
   if (nrhs < 1 || !X || !Y || ldx < h->n || ldy < h->n)
     return hm::fail(HM_ERR_INVALID, "hm_hmatvec_noalloc: bad vector arguments");
   hm::MatvecPlan& P = h->plan;
-  const size_t need = (size_t)P.t_per_rhs * (size_t)P.nrhs_cap;
+  const size_t need = (size_t)P.t_floats + (size_t)P.part_floats;
   if (need > hm::kNoallocScratchFloats)
     return hm::fail(HM_ERR_UNSUPPORTED,
                     "hm_hmatvec_noalloc: this matrix needs " + std::to_string(need) +
-                        " floats of projection scratch (sum of ranks x panel width); the static scratch holds " +
+                        " floats of projection scratch (sum of ranks x 16, plus chunk partials); the static scratch holds " +
                         std::to_string(hm::kNoallocScratchFloats) + " (16 MiB)");
   float* T = nullptr;
   HM_TRY(hm::noalloc_scratch(&T));
   cudaStream_t s = hm::as_stream(stream);
-  for (int c0 = 0; c0 < nrhs; c0 += P.nrhs_cap) {
-    const int nr = std::min(P.nrhs_cap, nrhs - c0);
-    const float* Xin = X + (size_t)c0 * ldx;
-    float* Yout = Y + (size_t)c0 * ldy;
-    // the scratch keeps the previous call's contents: the projections must start at zero
-    if (need > 0) HM_CUDA(cudaMemsetAsync(T, 0, sizeof(float) * need, s));
-    if (P.num_p1 > 0) {
-      hm::k_mv_project<<<P.num_p1, hm::kThreads, sizeof(float) * (hm::kMaxK * 33 + 32 * 33), s>>>(
-          reinterpret_cast<const int2*>(P.p1_items.p), P.lr.p, Xin, ldx, nr, T);
-      HM_LAUNCH_CHECK();
-    }
-    hm::k_mv_expand<<<P.num_leaves, hm::kThreads, hm::expand_smem(P.maxleaf, nr), s>>>(
-        h->tree->offsets.p, P.leaf_ptr.p, P.leaf_blk.p, P.lr.p, P.leaf_dptr.p, P.leaf_dblk.p, P.dense.p, T, Xin,
-        ldx, Yout, ldy, nr);
-    HM_LAUNCH_CHECK();
+  for (int c0 = 0; c0 < nrhs;) {
+    const int nr = std::min(16, nrhs - c0);
+    // the scratch keeps the previous call's contents: the projections that are
+    // summed must start at zero (run_panel clears them, the others are stored)
+    HM_TRY(hm::run_panel(h, nr, X + (size_t)c0 * ldx, ldx, Y + (size_t)c0 * ldy, ldy, T, s, nullptr));
+    c0 += nr;
   }
   return HM_OK;
 }
@@ -459,4 +508,30 @@ extern "C" hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, 
 extern "C" hm_status hm_hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, int ldx, float* Y, int ldy,
                                 int original_order, void* stream) {
   return hm::hmatvec(h, trans, nrhs, X, ldx, Y, ldy, original_order, hm::as_stream(stream));
+}
+
+extern "C" hm_status hm_hmatvec_profile(hm_hmatrix h, int nrhs, const float* X, int ldx, float* Y, int ldy,
+                                        void* stream, float* ms_project, float* ms_expand,
+                                        long long* bytes_project, long long* bytes_expand) {
+  if (!h) return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: null matrix");
+  if (nrhs < 1 || nrhs > 16 || !X || !Y || ldx < h->n || ldy < h->n)
+    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: need 1 <= nrhs <= 16 and valid vectors");
+  cudaStream_t s = hm::as_stream(stream);
+  cudaEvent_t e[3];
+  for (auto& x : e) HM_CUDA(cudaEventCreate(&x));
+  HM_CUDA(cudaEventRecord(e[0], s));
+  HM_TRY(hm::run_panel(h, nrhs, X, ldx, Y, ldy, h->plan.T.p, s, e[1]));
+  HM_CUDA(cudaEventRecord(e[2], s));
+  HM_CUDA(cudaEventSynchronize(e[2]));
+  float a = 0, b = 0;
+  HM_CUDA(cudaEventElapsedTime(&a, e[0], e[1]));
+  HM_CUDA(cudaEventElapsedTime(&b, e[1], e[2]));
+  for (auto& x : e) cudaEventDestroy(x);
+  if (ms_project) *ms_project = a;
+  if (ms_expand) *ms_expand = b;
+  long long bp = 0, be = 0;
+  hm::matvec_bytes(h, nrhs, &bp, &be);
+  if (bytes_project) *bytes_project = bp;
+  if (bytes_expand) *bytes_expand = be;
+  return HM_OK;
 }
