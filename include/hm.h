@@ -172,6 +172,8 @@ typedef struct {
   long long factor_bytes;    /* bytes of stored factors */
   long long dense_bytes;     /* bytes of stored dense blocks */
   long long num_unconverged; /* blocks above the leaf level left at their rank cap */
+  long long mixed_bytes;     /* mixed form: bytes one product reads from the BF16 copies
+                                (2 B per high part, 2 B per low part, both orientations) */
   double build_seconds;      /* device time of hm_hmatrix_build */
 } hm_hmatrix_stats;
 

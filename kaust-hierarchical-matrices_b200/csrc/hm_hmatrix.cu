@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <array>
 #include <numeric>
 #include <type_traits>
 
@@ -62,7 +63,7 @@ struct ProbState {
   int converged;
   int rounds;
   int r;      // rank after truncation (<= k)
-  int pad;
+  int rhi;    // mixed precision: columns [0, rhi) keep a BF16 low part
 };
 
 template <typename W>
@@ -680,7 +681,8 @@ __global__ void __launch_bounds__(kGramThreads) k_gram_big(const Prob* probs, co
 // leading r eigenvectors (columns in decreasing eigenvalue) to Wr (k x r, at
 // the same offset as G).
 __global__ void __launch_bounds__(kGramThreads) k_jacobi(const Prob* probs, ProbState* st, const long long* goff,
-                                                         const double* Gin, float* Wr, double tol2) {
+                                                         const double* Gin, float* Wr, double tol2,
+                                                         double rbudget) {
   extern __shared__ __align__(16) unsigned char jsm[];
   const int p = blockIdx.x;
   ProbState S = st[p];
@@ -689,6 +691,7 @@ __global__ void __launch_bounds__(kGramThreads) k_jacobi(const Prob* probs, Prob
   if (k <= 1) {
     if (t == 0) {
       st[p].r = k;
+      st[p].rhi = k;
       if (k == 1) Wr[goff[p]] = 1.f;
     }
     return;
@@ -795,6 +798,21 @@ __global__ void __launch_bounds__(kGramThreads) k_jacobi(const Prob* probs, Prob
     }
     r_sh = r;
     st[p].r = r;
+    // Mixed precision: column j of U V^T carries |u_j||v_j| = sigma_j; rounding
+    // both to BF16 perturbs it by at most ~2 * 2^-9 sigma_j.  The trailing
+    // columns whose rounding error fits rbudget keep only their BF16 high part.
+    int rhi = r;
+    if (rbudget > 0) {
+      double rt = 0;
+      const double c = 2.0 * 0x1p-18;  // (2^-9)^2 for each of u_j and v_j
+      while (rhi > 0) {
+        double l = fmax(G[order[rhi - 1] * kp + order[rhi - 1]], 0.0);
+        if (rt + c * l > rbudget * S.normA2) break;
+        rt += c * l;
+        --rhi;
+      }
+    }
+    st[p].rhi = rhi;
   }
   __syncthreads();
   const int r = r_sh;
@@ -843,6 +861,7 @@ size_t jacobi_smem(int kmax) {
   int kp = (kmax + 1) & ~1;
   return sizeof(double) * kp * kp + sizeof(float) * kp * kp + sizeof(double) * kp + sizeof(int) * 2 * kp + 64;
 }
+
 
 // ---------------------------------------------------------------------------
 // packing and dense blocks
@@ -971,7 +990,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   size_t freeb = 0, totb = 0;
   HM_CUDA(cudaMemGetInfo(&freeb, &totb));
   const size_t budget_bytes = std::min<size_t>(freeb / 4, (size_t)24 << 30);
-  std::vector<int> rank(nprob, 0), conv(nprob, 0);
+  std::vector<int> rank(nprob, 0), conv(nprob, 0), rhis(nprob, 0);
   std::vector<double> nrm(nprob, 0.0);
   long long pstart = 0;
   const double thresh2 = 0.09 * opt.tol * opt.tol;  // (0.3 tol)^2
@@ -1131,8 +1150,13 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       HM_LAUNCH_CHECK();
       HM_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)jacobi_smem(kMaxCols)));
-      k_jacobi<<<nb, kGramThreads, jacobi_smem(kbig), stream>>>(dprobs.p, dst.p, dgoff.p, Gbuf.p, Wr.p,
-                                                                 0.45 * opt.tol * opt.tol);
+      // error budget (relative, squared): sampling residual <= 0.09 tol^2 (the
+      // stopping test), truncation 0.45 tol^2 (FP32 form) or 0.35 tol^2 plus
+      // 0.15 tol^2 of BF16 rounding (mixed form)
+      const bool mixed = opt.precision == HM_PREC_MIXED;
+      k_jacobi<<<nb, kGramThreads, jacobi_smem(kbig), stream>>>(
+          dprobs.p, dst.p, dgoff.p, Gbuf.p, Wr.p, (mixed ? 0.35 : 0.45) * opt.tol * opt.tol,
+          mixed ? 0.15 * opt.tol * opt.tol : 0.0);
       HM_LAUNCH_CHECK();
       HM_CUDA(cudaMemcpyAsync(hst.data(), dst.p, sizeof(ProbState) * nb, cudaMemcpyDeviceToHost, stream));
       HM_CUDA(cudaStreamSynchronize(stream));
@@ -1157,6 +1181,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
           dv[i] = (long long)chunk_floats;
           chunk_floats += (size_t)P.n * S.r;
           rank[gi] = S.r;
+          rhis[gi] = std::min(S.rhi, S.r);
           conv[gi] = 1;
         } else {
           // the block and its mirror, each column-major, so every dense read in
@@ -1291,6 +1316,20 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       DenseBlock dt{P.c0, P.n, P.r0, P.m, 0, fdt[i]};
       h->h_dense.push_back(dt);
     }
+  }
+  // ---- mixed precision form -------------------------------------------------
+  if (opt.precision == HM_PREC_MIXED) {
+    std::vector<MxPair> mp;
+    for (long long i = 0; i < nprob; ++i) {
+      if (rank[i] <= 0) continue;
+      const Prob& P = probs[i];
+      mp.push_back(MxPair{P.level, P.r0, P.m, P.c0, P.n, rank[i], std::min(rhis[i], rank[i]), fu[i], fv[i]});
+    }
+    std::vector<MxDenseIn> md;
+    for (const DenseBlock& db : h->h_dense) md.push_back(MxDenseIn{db.r0, db.m, db.c0, db.n, db.D});
+    hm_status mst = mixed_build(h, mp, md, stream);
+    if (mst) return cleanup(mst);
+    h->stats.mixed_bytes = h->mx.store_tiles * 512;
   }
   h->stats.num_lowrank = lr_count;
   h->stats.num_dense = dense_count;

@@ -4,6 +4,7 @@
 
 #include "hm_internal.h"
 #include "hm_kernels.cuh"
+#include "hm_mixed.h"
 
 namespace hm {
 
@@ -69,6 +70,7 @@ struct hm_hmatrix_s {
   std::vector<hm::DevBuf<float>> storage;  // factor / dense chunks
   hm_hmatrix_stats stats{};
   hm::MatvecPlan plan;
+  hm::MxPlan mx;                     // mixed precision form (panels of BF16 hi + lo tiles)
   // host mirror of the block list (for export / tests)
   std::vector<hm::LRBlock> h_lr;
   std::vector<hm::DenseBlock> h_dense;

@@ -275,6 +275,7 @@ __global__ void k_scatter_rows(const float* Yp, const int* perm, int n, int nrhs
 // scratch (16 x kpad per block, then the chunk partials).
 hm_status run_panel(hm_hmatrix h, int nr, const float* X, int ldx, float* Y, int ldy, float* T, cudaStream_t s,
                     cudaEvent_t e_mid) {
+  if (h->mx.enabled) return mixed_run_panel(h, nr, X, ldx, Y, ldy, T, s, e_mid);
   MatvecPlan& P = h->plan;
   float* Tpart = T + P.t_floats;
   if (P.num_p1 > 0) {
@@ -379,7 +380,9 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   HM_TRY(P.dense.alloc(std::max<size_t>(h->h_dense.size(), 1)));
   HM_TRY(P.leaf_dptr.alloc(nleaf + 1));
   HM_TRY(P.leaf_dblk.alloc(dblk.size()));
-  HM_TRY(P.T.alloc(std::max<long long>(tk + part, 1)));
+  // projection scratch of one 16-column panel, for whichever form runs
+  const long long scratch = h->mx.enabled ? h->mx.scratch_floats() : tk + part;
+  HM_TRY(P.T.alloc(std::max<long long>(scratch, 1)));
   HM_TRY(P.Xp.alloc((size_t)h->n * nrhs_cap));
   HM_TRY(P.Yp.alloc((size_t)h->n * nrhs_cap));
   auto up = [&](void* dst, const void* src, size_t bytes) -> hm_status {
@@ -439,11 +442,18 @@ hm_status hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, int ldx, fl
 // blocks read once, X read once and Y written once per phase that touches them.
 void matvec_bytes(hm_hmatrix h, int nrhs, long long* b_project, long long* b_expand) {
   long long p1 = 0, p2 = 0;
-  for (const auto& b : h->h_lr) {
-    p1 += 4ll * b.n * b.k;
-    p2 += 4ll * b.m * b.k;
+  if (h->mx.enabled) {
+    // BF16 high parts of every factor column plus the low parts of the
+    // columns that keep one (unpadded); dense blocks hi + lo
+    p1 = h->mx.bytes_p1;
+    p2 = h->mx.bytes_p2;
+  } else {
+    for (const auto& b : h->h_lr) {
+      p1 += 4ll * b.n * b.k;
+      p2 += 4ll * b.m * b.k;
+    }
+    for (const auto& d : h->h_dense) p2 += 4ll * d.m * d.n;
   }
-  for (const auto& d : h->h_dense) p2 += 4ll * d.m * d.n;
   p1 += 4ll * h->n * nrhs;      // X
   p2 += 4ll * h->n * nrhs * 2;  // X (dense blocks) and Y
   *b_project = p1;
@@ -486,7 +496,7 @@ extern "C" hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, 
   if (nrhs < 1 || !X || !Y || ldx < h->n || ldy < h->n)
     return hm::fail(HM_ERR_INVALID, "hm_hmatvec_noalloc: bad vector arguments");
   hm::MatvecPlan& P = h->plan;
-  const size_t need = (size_t)P.t_floats + (size_t)P.part_floats;
+  const size_t need = h->mx.enabled ? (size_t)h->mx.scratch_floats() : (size_t)P.t_floats + (size_t)P.part_floats;
   if (need > hm::kNoallocScratchFloats)
     return hm::fail(HM_ERR_UNSUPPORTED,
                     "hm_hmatvec_noalloc: this matrix needs " + std::to_string(need) +

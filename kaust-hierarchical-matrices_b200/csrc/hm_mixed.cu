@@ -1,0 +1,622 @@
+// hm_mixed.cu -- mixed-precision H-matvec: BF16 hi + lo factor panels on the
+// tensor cores (mma.sync m16n8k16, FP32 accumulation).
+//
+// One product of <= 16 right-hand sides runs four kernels:
+//   k_mx_split_x  X (FP32, tree order) -> BF16 hi + lo fragments per 32-row tile
+//   k_mx_p1       S = panel^T X per (panel, column group, row chunk)
+//   k_mx_gather   T = S summed over row chunks, each column moved to the panel
+//                 that expands it (the mirror block's factor), split hi + lo
+//   k_mx_p2       Y = sum over the ancestors' panels of U T, plus dense blocks
+// Each product of a BF16 pair uses three MMAs (hi*lo, lo*hi, hi*hi; lo*lo is
+// below FP32 rounding); the low-part MMA of a factor is skipped for the tiles
+// that carry none.  The tensor core's internal sums do not round to nearest, so
+// each short chain of MMAs goes into a zeroed temporary that is added to the
+// running FP32 sum with an ordinary FADD.
+#include <algorithm>
+#include <vector>
+
+#include "hm_hmatrix.h"
+#include "hm_mixed.h"
+#include "hm_mma.cuh"
+
+namespace hm {
+namespace {
+
+constexpr int kChunkTiles = 64;  // row tiles (2048 rows) per phase-1 unit
+constexpr int kGroupTiles = 8;   // column tiles per phase-1 unit
+
+__device__ __forceinline__ void mma_a4(float (&d)[4], const uint4& a, uint32_t b0, uint32_t b1) {
+  mma_bf16(d, a.x, a.y, a.z, a.w, b0, b1);
+}
+
+// ---- X -> fragments ---------------------------------------------------------
+// Xf[tile][part][lane], part 0/1 = hi of rows 0-15 / 16-31, part 2/3 = lo:
+// the m16n8k16 A fragment of X^T (16 right-hand sides x 16 rows):
+//   {X[2t,2t+1][g], X[2t,2t+1][g+8], X[2t+8,2t+9][g], X[2t+8,2t+9][g+8]}
+__global__ void __launch_bounds__(128) k_mx_split_x(const float* __restrict__ X, int ldx, int nr, int num_tiles,
+                                                    const int* __restrict__ tile_leaf,
+                                                    const int* __restrict__ leaf_tile0,
+                                                    const int* __restrict__ leaf_off, uint4* __restrict__ Xf) {
+  __shared__ float xs[4][16][33];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int G = blockIdx.x * 4 + w;
+  if (G >= num_tiles) return;  // whole warp; only warp-level syncs below
+  const int x = tile_leaf[G];
+  const int row = leaf_off[x] + 32 * (G - leaf_tile0[x]) + lane;
+  const bool ok = row < leaf_off[x + 1];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) xs[w][r][lane] = (ok && r < nr) ? __ldg(X + (size_t)r * ldx + row) : 0.f;
+  __syncwarp();
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const int i0 = 16 * s + 2 * t;
+    uint4 hi, lo;
+    split_bf16x2(xs[w][g][i0], xs[w][g][i0 + 1], hi.x, lo.x);
+    split_bf16x2(xs[w][g + 8][i0], xs[w][g + 8][i0 + 1], hi.y, lo.y);
+    split_bf16x2(xs[w][g][i0 + 8], xs[w][g][i0 + 9], hi.z, lo.z);
+    split_bf16x2(xs[w][g + 8][i0 + 8], xs[w][g + 8][i0 + 9], hi.w, lo.w);
+    Xf[((size_t)G * 4 + s) * 32 + lane] = hi;
+    Xf[((size_t)G * 4 + 2 + s) * 32 + lane] = lo;
+  }
+}
+
+// ---- phase 1 ----------------------------------------------------------------
+// C (16 right-hand sides x 8 columns) per column tile = X^T V over the unit's
+// row tiles.  NCT: column tiles compiled for, RU: row tiles loaded per step.
+template <int NCT, int RU>
+__device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, const uint4* __restrict__ store,
+                                           const uint4* __restrict__ Xf, float4* __restrict__ S, int lane) {
+  float acc[NCT][4];
+#pragma unroll
+  for (int j = 0; j < NCT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+  for (int r = 0; r < u.nrt; r += RU) {
+    uint4 xf[RU][4], vh[RU][NCT], vl[RU][NCT];
+#pragma unroll
+    for (int q = 0; q < RU; ++q) {
+      const bool ok = r + q < u.nrt;
+      const long long rt = u.rt0 + r + q;
+      const uint4* xp = Xf + (size_t)(P.tile0 + rt) * 128 + lane;
+#pragma unroll
+      for (int p = 0; p < 4; ++p) xf[q][p] = ok ? __ldg(xp + p * 32) : z;
+      const uint4* hp = store + (P.hi1 + rt * P.nct + u.ct0) * 32 + lane;
+      const uint4* lp = store + (P.lo1 + rt * P.nctl + u.ct0) * 32 + lane;
+#pragma unroll
+      for (int j = 0; j < NCT; ++j) {
+        vh[q][j] = ok && j < u.nct ? __ldcs(hp + j * 32) : z;
+        vl[q][j] = ok && j < u.nct && u.ct0 + j < P.nctl ? __ldcs(lp + j * 32) : z;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < RU; ++q) {
+      if (r + q < u.nrt) {
+#pragma unroll
+        for (int j = 0; j < NCT; ++j) {
+          if (j < u.nct) {
+            float d[4] = {0.f, 0.f, 0.f, 0.f};
+            mma_a4(d, xf[q][2], vh[q][j].x, vh[q][j].y);  // X_lo V_hi
+            mma_a4(d, xf[q][3], vh[q][j].z, vh[q][j].w);
+            if (u.ct0 + j < P.nctl) {                     // X_hi V_lo
+              mma_a4(d, xf[q][0], vl[q][j].x, vl[q][j].y);
+              mma_a4(d, xf[q][1], vl[q][j].z, vl[q][j].w);
+            }
+            mma_a4(d, xf[q][0], vh[q][j].x, vh[q][j].y);  // X_hi V_hi
+            mma_a4(d, xf[q][1], vh[q][j].z, vh[q][j].w);
+            add4(acc[j], d);
+          }
+        }
+      }
+    }
+  }
+  float4* out = S + (P.s0 + (long long)u.chunk * P.nct + u.ct0) * 32 + lane;
+#pragma unroll
+  for (int j = 0; j < NCT; ++j)
+    if (j < u.nct) out[j * 32] = make_float4(acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+}
+
+__global__ void __launch_bounds__(128) k_mx_p1(const MxUnit* __restrict__ units, int nunits,
+                                               const MxPanel* __restrict__ panels, const uint4* __restrict__ store,
+                                               const uint4* __restrict__ Xf, float4* __restrict__ S) {
+  const int w = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (w >= nunits) return;
+  const int lane = threadIdx.x & 31;
+  const MxUnit u = units[w];
+  const MxPanel P = panels[u.panel];
+  if (u.nct > 4)
+    mx_p1_unit<8, 1>(u, P, store, Xf, S, lane);
+  else if (u.nct > 2)
+    mx_p1_unit<4, 2>(u, P, store, Xf, S, lane);
+  else
+    mx_p1_unit<2, 4>(u, P, store, Xf, S, lane);
+}
+
+// ---- column gather ----------------------------------------------------------
+// T tile word of lane (g,t) = {hi(T[2t][g], T[2t+1][g]), hi(.. g+8), lo(.. g), lo(.. g+8)}
+// where T[c][r] = sum over the source panel's row chunks of S[source column][r].
+// S tile: lane (g,t) = {C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1]}.
+__global__ void k_mx_gather(const int2* __restrict__ tsrc, long long t_tiles, const MxPanel* __restrict__ panels,
+                            const float* __restrict__ S, uint4* __restrict__ T) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= t_tiles * 32) return;
+  const long long tile = i >> 5;
+  const int lane = (int)(i & 31), g = lane >> 2, t = lane & 3;
+  float v[2][2];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const int2 src = __ldg(tsrc + tile * 8 + 2 * t + c);
+    float a = 0.f, b = 0.f;
+    if (src.x >= 0) {
+      const MxPanel& P = panels[src.x];
+      const int cc = src.y;
+      const long long base = (P.s0 + (cc >> 3)) * 128 + (4 * g + ((cc & 7) >> 1)) * 4 + (cc & 1);
+      const long long stride = (long long)P.nct * 128;
+      for (int ch = 0; ch < P.nchunk; ++ch) {
+        a += __ldg(S + base + ch * stride);
+        b += __ldg(S + base + ch * stride + 2);
+      }
+    }
+    v[c][0] = a;
+    v[c][1] = b;
+  }
+  uint4 o;
+  split_bf16x2(v[0][0], v[1][0], o.x, o.z);
+  split_bf16x2(v[0][1], v[1][1], o.y, o.w);
+  T[i] = o;
+}
+
+// ---- phase 2 ----------------------------------------------------------------
+// acc[mt][nb] += A (16 rows x 16 columns, tiles h0|h1 + l0|l1) B (16 x 8)
+__device__ __forceinline__ void mx_p2_step(float (&acc)[2][2][4], const uint4& h0, const uint4& h1,
+                                           const uint4& l0, const uint4& l1, const uint32_t (&bh)[2][2],
+                                           const uint32_t (&bl)[2][2], bool lo) {
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt) {
+    const uint32_t a0 = mt ? h0.z : h0.x, a1 = mt ? h0.w : h0.y, a2 = mt ? h1.z : h1.x, a3 = mt ? h1.w : h1.y;
+    const uint32_t c0 = mt ? l0.z : l0.x, c1 = mt ? l0.w : l0.y, c2 = mt ? l1.z : l1.x, c3 = mt ? l1.w : l1.y;
+#pragma unroll
+    for (int nb = 0; nb < 2; ++nb) {
+      float d[4] = {0.f, 0.f, 0.f, 0.f};
+      mma_bf16(d, a0, a1, a2, a3, bl[nb][0], bl[nb][1]);
+      if (lo) mma_bf16(d, c0, c1, c2, c3, bh[nb][0], bh[nb][1]);
+      mma_bf16(d, a0, a1, a2, a3, bh[nb][0], bh[nb][1]);
+      add4(acc[mt][nb], d);
+    }
+  }
+}
+
+// One warp per global row tile (32 rows of one leaf): every ancestor cluster's
+// panel rows times its T, then the dense blocks of the leaf row.
+__global__ void __launch_bounds__(128) k_mx_p2(int num_tiles, int depth, const int* __restrict__ tile_leaf,
+                                               const int* __restrict__ leaf_tile0, const int* __restrict__ leaf_off,
+                                               const int* __restrict__ pan_of, const MxPanel* __restrict__ panels,
+                                               const uint4* __restrict__ store, const uint4* __restrict__ T,
+                                               const int* __restrict__ leaf_dptr, const int* __restrict__ leaf_dblk,
+                                               const MxDense* __restrict__ dense, const uint4* __restrict__ Xf,
+                                               float* __restrict__ Y, int ldy, int nr) {
+  const int G = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (G >= num_tiles) return;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int x = tile_leaf[G];
+  float acc[2][2][4];
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nb = 0; nb < 2; ++nb) acc[mt][nb][0] = acc[mt][nb][1] = acc[mt][nb][2] = acc[mt][nb][3] = 0.f;
+  const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+  for (int l = 1; l <= depth; ++l) {
+    const int p = __ldg(pan_of + (1 << l) - 1 + (x >> (depth - l)));
+    if (p < 0) continue;
+    const MxPanel P = panels[p];
+    const long long rt = G - P.tile0;
+    const uint4* uh = store + (P.hi2 + rt * P.nct) * 32 + lane;
+    const uint4* ul = store + (P.lo2 + rt * P.nctl) * 32 + lane;
+    const uint4* tt = T + P.t0 * 32 + lane;
+#pragma unroll 2
+    for (int ct = 0; ct < P.nct; ct += 2) {
+      const bool two = ct + 1 < P.nct, lo0 = ct < P.nctl, lo1 = ct + 1 < P.nctl;
+      const uint4 h0 = __ldcs(uh + ct * 32);
+      const uint4 h1 = two ? __ldcs(uh + (ct + 1) * 32) : z;
+      const uint4 l0 = lo0 ? __ldcs(ul + ct * 32) : z;
+      const uint4 l1 = lo1 ? __ldcs(ul + (ct + 1) * 32) : z;
+      const uint4 t0 = __ldg(tt + ct * 32);
+      const uint4 t1 = two ? __ldg(tt + (ct + 1) * 32) : z;
+      const uint32_t bh[2][2] = {{t0.x, t1.x}, {t0.y, t1.y}};
+      const uint32_t bl[2][2] = {{t0.z, t1.z}, {t0.w, t1.w}};
+      mx_p2_step(acc, h0, h1, l0, l1, bh, bl, lo0);
+    }
+  }
+  for (int q = leaf_dptr[x]; q < leaf_dptr[x + 1]; ++q) {
+    const MxDense D = dense[leaf_dblk[q]];
+    const long long rt = G - D.row_tile0;
+    const uint4* dh = store + (D.hi + rt * D.nct) * 32 + lane;
+    const uint4* dl = store + (D.lo + rt * D.nct) * 32 + lane;
+    for (int ct = 0; ct < D.nct; ct += 2) {
+      const uint4 h0 = __ldcs(dh + ct * 32), h1 = __ldcs(dh + (ct + 1) * 32);
+      const uint4 l0 = __ldcs(dl + ct * 32), l1 = __ldcs(dl + (ct + 1) * 32);
+      const size_t xt = (size_t)(D.col_tile0 + (ct >> 2)) * 128 + (size_t)((ct >> 1) & 1) * 32 + lane;
+      const uint4 xh = __ldg(Xf + xt), xl = __ldg(Xf + xt + 64);
+      const uint32_t bh[2][2] = {{xh.x, xh.z}, {xh.y, xh.w}};
+      const uint32_t bl[2][2] = {{xl.x, xl.z}, {xl.y, xl.w}};
+      mx_p2_step(acc, h0, h1, l0, l1, bh, bl, true);
+    }
+  }
+  const int base = leaf_off[x] + 32 * (G - leaf_tile0[x]);
+  const int lim = leaf_off[x + 1];
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nb = 0; nb < 2; ++nb) {
+      const int ra = base + 16 * mt + g, rb = ra + 8, c = 8 * nb + 2 * t;
+      if (c < nr) {
+        if (ra < lim) Y[(size_t)c * ldy + ra] = acc[mt][nb][0];
+        if (rb < lim) Y[(size_t)c * ldy + rb] = acc[mt][nb][2];
+      }
+      if (c + 1 < nr) {
+        if (ra < lim) Y[(size_t)(c + 1) * ldy + ra] = acc[mt][nb][1];
+        if (rb < lim) Y[(size_t)(c + 1) * ldy + rb] = acc[mt][nb][3];
+      }
+    }
+}
+
+// ---- conversion (build time) ------------------------------------------------
+__device__ __forceinline__ int find_item(const long long* start, int n, long long w) {
+  int lo = 0, hi = n - 1;  // largest i with start[i] <= w
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (start[mid] <= w)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// One warp per 32 x 8 panel tile: both fragment orders, hi and (for the
+// leading tiles) lo.  colsrc: per panel column, the FP32 factor column over
+// the cluster's rows, or null for a padding column.
+__global__ void k_mx_conv_panels(const MxPanel* __restrict__ panels, const long long* __restrict__ unit_start,
+                                 int npanels, long long nunits, const float* const* __restrict__ colsrc,
+                                 const int* __restrict__ tile_leaf, const int* __restrict__ leaf_tile0,
+                                 const int* __restrict__ leaf_off, uint4* __restrict__ store) {
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= nunits) return;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int pi = find_item(unit_start, npanels, w);
+  const MxPanel P = panels[pi];
+  const long long local = w - unit_start[pi];
+  const int rt = (int)(local / P.nct), ct = (int)(local % P.nct);
+  const int G = P.tile0 + rt;
+  const int x = tile_leaf[G];
+  const int rbase = leaf_off[x] + 32 * (G - leaf_tile0[x]) - P.r0;
+  const int rlim = leaf_off[x + 1] - P.r0;
+  const float* const* cs = colsrc + P.t0 * 8;
+  auto val = [&](int r, int c) -> float {
+    const float* col = cs[c];
+    const int lr = rbase + r;
+    return (col != nullptr && lr < rlim) ? col[lr] : 0.f;
+  };
+  uint4 h1, l1, h2, l2;
+  const int cp1 = 8 * ct + g;
+  split_bf16x2(val(2 * t, cp1), val(2 * t + 1, cp1), h1.x, l1.x);
+  split_bf16x2(val(2 * t + 8, cp1), val(2 * t + 9, cp1), h1.y, l1.y);
+  split_bf16x2(val(2 * t + 16, cp1), val(2 * t + 17, cp1), h1.z, l1.z);
+  split_bf16x2(val(2 * t + 24, cp1), val(2 * t + 25, cp1), h1.w, l1.w);
+  const int cp2 = 8 * ct + 2 * t;
+  split_bf16x2(val(g, cp2), val(g, cp2 + 1), h2.x, l2.x);
+  split_bf16x2(val(g + 8, cp2), val(g + 8, cp2 + 1), h2.y, l2.y);
+  split_bf16x2(val(g + 16, cp2), val(g + 16, cp2 + 1), h2.z, l2.z);
+  split_bf16x2(val(g + 24, cp2), val(g + 24, cp2 + 1), h2.w, l2.w);
+  store[(P.hi1 + (long long)rt * P.nct + ct) * 32 + lane] = h1;
+  store[(P.hi2 + (long long)rt * P.nct + ct) * 32 + lane] = h2;
+  if (ct < P.nctl) {
+    store[(P.lo1 + (long long)rt * P.nctl + ct) * 32 + lane] = l1;
+    store[(P.lo2 + (long long)rt * P.nctl + ct) * 32 + lane] = l2;
+  }
+}
+
+// One warp per 32 x 8 tile of a dense block (P2 order, hi + lo)
+__global__ void k_mx_conv_dense(const MxDense* __restrict__ dense, const long long* __restrict__ unit_start,
+                                int ndense, long long nunits, const int* __restrict__ tile_leaf,
+                                const int* __restrict__ leaf_tile0, const int* __restrict__ leaf_off,
+                                uint4* __restrict__ store) {
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= nunits) return;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int di = find_item(unit_start, ndense, w);
+  const MxDense D = dense[di];
+  const long long local = w - unit_start[di];
+  const int rt = (int)(local / D.nct), ct = (int)(local % D.nct);
+  const int G = D.row_tile0 + rt;
+  const int x = tile_leaf[G];
+  const int rbase = leaf_off[x] + 32 * (G - leaf_tile0[x]) - D.r0;
+  const int rlim = leaf_off[x + 1] - D.r0;
+  const int pc = 8 * ct + 2 * t;  // padded column (even; pc and pc + 1 share a 32-column tile)
+  const int GC = D.col_tile0 + (pc >> 5);
+  const int y = tile_leaf[GC];
+  const int cbase = leaf_off[y] + 32 * (GC - leaf_tile0[y]) - D.c0 + (pc & 31);
+  const int clim = leaf_off[y + 1] - D.c0;
+  auto val = [&](int r, int c) -> float {
+    const int lr = rbase + r;
+    return (lr < rlim && c < clim) ? D.src[(size_t)c * D.m + lr] : 0.f;
+  };
+  uint4 h, l;
+  split_bf16x2(val(g, cbase), val(g, cbase + 1), h.x, l.x);
+  split_bf16x2(val(g + 8, cbase), val(g + 8, cbase + 1), h.y, l.y);
+  split_bf16x2(val(g + 16, cbase), val(g + 16, cbase + 1), h.z, l.z);
+  split_bf16x2(val(g + 24, cbase), val(g + 24, cbase + 1), h.w, l.w);
+  store[(D.hi + (long long)rt * D.nct + ct) * 32 + lane] = h;
+  store[(D.lo + (long long)rt * D.nct + ct) * 32 + lane] = l;
+}
+
+template <class T>
+hm_status upload(DevBuf<T>& b, const std::vector<T>& v, cudaStream_t s) {
+  HM_TRY(b.alloc(std::max<size_t>(v.size(), 1)));
+  if (!v.empty()) HM_CUDA(cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+  return HM_OK;
+}
+
+}  // namespace
+
+hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const std::vector<MxDenseIn>& dense_in,
+                      cudaStream_t s) {
+  MxPlan& M = h->mx;
+  const int depth = h->depth;
+  const std::vector<int>& lo = h->tree->h_offsets;
+  const int nleaf = 1 << depth;
+
+  // global 32-row tiles, padded per leaf
+  std::vector<int> leaf_tile0(nleaf + 1), tile_leaf;
+  for (int x = 0; x < nleaf; ++x) {
+    leaf_tile0[x] = (int)tile_leaf.size();
+    const int nt = (lo[x + 1] - lo[x] + 31) / 32;
+    for (int i = 0; i < nt; ++i) tile_leaf.push_back(x);
+  }
+  leaf_tile0[nleaf] = (int)tile_leaf.size();
+  M.num_tiles = (int)tile_leaf.size();
+
+  // leaf range [first, end) of the cluster whose rows are [r0, r0 + m)
+  auto leaf_range = [&](int r0, int m, int* first, int* end) {
+    *first = (int)(std::lower_bound(lo.begin(), lo.end() - 1, r0) - lo.begin());
+    *end = (int)(std::lower_bound(lo.begin(), lo.end() - 1, r0 + m) - lo.begin());
+  };
+  // the level-l cluster with rows [r0, r0 + m) (m > 0)
+  auto cluster_of = [&](int level, int r0, int m) -> int {
+    const int sh = depth - level;
+    int a = 0, b = (1 << level) - 1;  // first a with lo[a << sh] >= r0
+    while (a < b) {
+      const int mid = (a + b) >> 1;
+      if (lo[(size_t)mid << sh] < r0)
+        a = mid + 1;
+      else
+        b = mid;
+    }
+    while (a + 1 < (1 << level) && lo[(size_t)(a + 1) << sh] - r0 < m) ++a;  // skip empty clusters
+    return a;
+  };
+
+  // ---- panels ----------------------------------------------------------------
+  std::vector<int> pan_of(((size_t)2 << depth) - 1, -1);
+  struct Side {
+    int pair, side;  // side 0: fu (row cluster), 1: fv (column cluster)
+  };
+  std::vector<std::vector<Side>> members;
+  std::vector<int> plevel, pcl;
+  std::vector<int> panel_u(pairs.size(), -1), panel_v(pairs.size(), -1);
+  for (size_t i = 0; i < pairs.size(); ++i) {
+    const MxPair& q = pairs[i];
+    if (q.k <= 0) continue;
+    for (int side = 0; side < 2; ++side) {
+      const int a = side ? cluster_of(q.level, q.c0, q.n) : cluster_of(q.level, q.r0, q.m);
+      const size_t id = ((size_t)1 << q.level) - 1 + a;
+      if (pan_of[id] < 0) {
+        pan_of[id] = (int)members.size();
+        members.emplace_back();
+        plevel.push_back(q.level);
+        pcl.push_back(a);
+      }
+      members[pan_of[id]].push_back(Side{(int)i, side});
+      (side ? panel_v : panel_u)[i] = pan_of[id];
+    }
+  }
+  const int np = (int)members.size();
+  std::vector<MxPanel> panels(np);
+  std::vector<int> colL_u(pairs.size()), colH_u(pairs.size()), colL_v(pairs.size()), colH_v(pairs.size());
+  long long tiles = 0, s_tiles = 0, t_tiles = 0;
+  for (int p = 0; p < np; ++p) {
+    long long sl = 0, sh_ = 0;
+    for (const Side& m : members[p]) {
+      sl += pairs[m.pair].khi;
+      sh_ += pairs[m.pair].k - pairs[m.pair].khi;
+    }
+    const int KL = (int)((sl + 7) / 8 * 8), KH = (int)((sh_ + 7) / 8 * 8);
+    long long al = 0, ah = KL;
+    for (const Side& m : members[p]) {
+      const MxPair& q = pairs[m.pair];
+      (m.side ? colL_v : colL_u)[m.pair] = (int)al;
+      (m.side ? colH_v : colH_u)[m.pair] = (int)ah;
+      al += q.khi;
+      ah += q.k - q.khi;
+    }
+    MxPanel& P = panels[p];
+    const int sh = depth - plevel[p];
+    const int x0 = pcl[p] << sh, x1 = (pcl[p] + 1) << sh;
+    P.nct = (KL + KH) / 8;
+    P.nctl = KL / 8;
+    P.tile0 = leaf_tile0[x0];
+    P.nrt = leaf_tile0[x1] - P.tile0;
+    P.r0 = lo[x0];
+    P.nchunk = std::max(1, (P.nrt + kChunkTiles - 1) / kChunkTiles);
+    P.hi1 = tiles;
+    tiles += (long long)P.nrt * P.nct;
+    P.lo1 = tiles;
+    tiles += (long long)P.nrt * P.nctl;
+    P.hi2 = tiles;
+    tiles += (long long)P.nrt * P.nct;
+    P.lo2 = tiles;
+    tiles += (long long)P.nrt * P.nctl;
+    P.s0 = s_tiles;
+    s_tiles += (long long)P.nchunk * P.nct;
+    P.t0 = t_tiles;
+    t_tiles += P.nct;
+  }
+
+  // column sources and the projection's column map
+  std::vector<const float*> colsrc((size_t)t_tiles * 8, nullptr);
+  std::vector<int2> tsrc((size_t)t_tiles * 8, make_int2(-1, -1));
+  long long bytes_lr = 0;
+  for (size_t i = 0; i < pairs.size(); ++i) {
+    const MxPair& q = pairs[i];
+    if (q.k <= 0) continue;
+    const int pu = panel_u[i], pv = panel_v[i];
+    const long long bu = panels[pu].t0 * 8, bv = panels[pv].t0 * 8;
+    for (int c = 0; c < q.k; ++c) {
+      const int cu = c < q.khi ? colL_u[i] + c : colH_u[i] + c - q.khi;
+      const int cv = c < q.khi ? colL_v[i] + c : colH_v[i] + c - q.khi;
+      colsrc[bu + cu] = q.fu + (size_t)c * q.m;
+      colsrc[bv + cv] = q.fv + (size_t)c * q.n;
+      tsrc[bu + cu] = make_int2(pv, cv);  // Y_u += fu (fv^T X_v)
+      tsrc[bv + cv] = make_int2(pu, cu);  // Y_v += fv (fu^T X_u)
+    }
+    bytes_lr += 2ll * (q.m + q.n) * (q.k + q.khi);
+  }
+
+  // phase-1 units, the largest first
+  std::vector<MxUnit> units;
+  for (int p = 0; p < np; ++p) {
+    const MxPanel& P = panels[p];
+    for (int c = 0; c < P.nct; c += kGroupTiles)
+      for (int ch = 0; ch < P.nchunk; ++ch)
+        units.push_back(MxUnit{p, c, std::min(kGroupTiles, P.nct - c), ch * kChunkTiles,
+                               std::min(kChunkTiles, P.nrt - ch * kChunkTiles), ch});
+  }
+  std::stable_sort(units.begin(), units.end(),
+                   [](const MxUnit& a, const MxUnit& b) { return a.nrt * a.nct > b.nrt * b.nct; });
+
+  // ---- dense blocks ----------------------------------------------------------
+  std::vector<MxDense> dense;
+  std::vector<std::vector<int>> leaf_d(nleaf);
+  long long bytes_dense = 0;
+  for (const MxDenseIn& di : dense_in) {
+    if (di.m <= 0 || di.n <= 0) continue;
+    int xs, xe, ys, ye;
+    leaf_range(di.r0, di.m, &xs, &xe);
+    leaf_range(di.c0, di.n, &ys, &ye);
+    MxDense D{};
+    D.row_tile0 = leaf_tile0[xs];
+    D.nrt = leaf_tile0[xe] - D.row_tile0;
+    D.col_tile0 = leaf_tile0[ys];
+    D.nct = 4 * (leaf_tile0[ye] - D.col_tile0);
+    D.r0 = di.r0;
+    D.c0 = di.c0;
+    D.m = di.m;
+    D.n = di.n;
+    D.src = di.D;
+    D.hi = tiles;
+    tiles += (long long)D.nrt * D.nct;
+    D.lo = tiles;
+    tiles += (long long)D.nrt * D.nct;
+    for (int x = xs; x < xe; ++x) leaf_d[x].push_back((int)dense.size());
+    dense.push_back(D);
+    bytes_dense += 4ll * di.m * di.n;
+  }
+  std::vector<int> dptr(nleaf + 1, 0), dblk;
+  for (int x = 0; x < nleaf; ++x) {
+    dptr[x] = (int)dblk.size();
+    dblk.insert(dblk.end(), leaf_d[x].begin(), leaf_d[x].end());
+  }
+  dptr[nleaf] = (int)dblk.size();
+
+  // ---- upload and convert ----------------------------------------------------
+  M.store_tiles = tiles;
+  HM_TRY(M.store.alloc((size_t)std::max<long long>(tiles, 1) * 32));
+  HM_TRY(upload(M.panels, panels, s));
+  HM_TRY(upload(M.pan_of, pan_of, s));
+  HM_TRY(upload(M.units, units, s));
+  HM_TRY(upload(M.tile_leaf, tile_leaf, s));
+  HM_TRY(upload(M.leaf_tile0, leaf_tile0, s));
+  HM_TRY(upload(M.tsrc, tsrc, s));
+  HM_TRY(upload(M.dense, dense, s));
+  HM_TRY(upload(M.leaf_dptr, dptr, s));
+  HM_TRY(upload(M.leaf_dblk, dblk, s));
+  M.num_panels = np;
+  M.num_units = (int)units.size();
+  M.num_dense = (int)dense.size();
+  M.s_tiles = s_tiles;
+  M.t_tiles = t_tiles;
+  // each factor is read once per phase (as V of one orientation in phase 1,
+  // as U of the other in phase 2)
+  M.bytes_p1 = bytes_lr;
+  M.bytes_p2 = bytes_lr + bytes_dense;
+
+  DevBuf<const float*> dcol;
+  DevBuf<long long> dstart;
+  if (np > 0) {
+    std::vector<long long> start(np);
+    long long tot = 0;
+    for (int p = 0; p < np; ++p) {
+      start[p] = tot;
+      tot += (long long)panels[p].nrt * panels[p].nct;
+    }
+    HM_TRY(upload(dcol, colsrc, s));
+    HM_TRY(upload(dstart, start, s));
+    if (tot > 0) {
+      k_mx_conv_panels<<<(unsigned)((tot * 32 + 255) / 256), 256, 0, s>>>(
+          M.panels.p, dstart.p, np, tot, dcol.p, M.tile_leaf.p, M.leaf_tile0.p, h->tree->offsets.p, M.store.p);
+      HM_LAUNCH_CHECK();
+    }
+    HM_CUDA(cudaStreamSynchronize(s));
+  }
+  if (!dense.empty()) {
+    std::vector<long long> start(dense.size());
+    long long tot = 0;
+    for (size_t i = 0; i < dense.size(); ++i) {
+      start[i] = tot;
+      tot += (long long)dense[i].nrt * dense[i].nct;
+    }
+    DevBuf<long long> ds;
+    HM_TRY(upload(ds, start, s));
+    if (tot > 0) {
+      k_mx_conv_dense<<<(unsigned)((tot * 32 + 255) / 256), 256, 0, s>>>(
+          M.dense.p, ds.p, (int)dense.size(), tot, M.tile_leaf.p, M.leaf_tile0.p, h->tree->offsets.p, M.store.p);
+      HM_LAUNCH_CHECK();
+    }
+    HM_CUDA(cudaStreamSynchronize(s));
+  }
+  HM_CUDA(cudaStreamSynchronize(s));
+  M.enabled = true;
+  return HM_OK;
+}
+
+hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, float* scratch,
+                          cudaStream_t s, cudaEvent_t e_mid) {
+  MxPlan& M = h->mx;
+  uint4* Xf = reinterpret_cast<uint4*>(scratch);
+  float* S = scratch + (size_t)M.num_tiles * 4 * 128;
+  uint4* T = reinterpret_cast<uint4*>(S + (size_t)M.s_tiles * 128);
+  const int* leaf_off = h->tree->offsets.p;
+  if (M.num_tiles > 0) {
+    k_mx_split_x<<<(M.num_tiles + 3) / 4, 128, 0, s>>>(X, ldx, nr, M.num_tiles, M.tile_leaf.p, M.leaf_tile0.p,
+                                                       leaf_off, Xf);
+    HM_LAUNCH_CHECK();
+  }
+  if (M.num_units > 0) {
+    k_mx_p1<<<(M.num_units + 3) / 4, 128, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf,
+                                                  reinterpret_cast<float4*>(S));
+    HM_LAUNCH_CHECK();
+  }
+  if (M.t_tiles > 0) {
+    k_mx_gather<<<(unsigned)((M.t_tiles * 32 + 255) / 256), 256, 0, s>>>(M.tsrc.p, M.t_tiles, M.panels.p, S, T);
+    HM_LAUNCH_CHECK();
+  }
+  if (e_mid) HM_CUDA(cudaEventRecord(e_mid, s));
+  if (M.num_tiles > 0) {
+    k_mx_p2<<<(M.num_tiles + 3) / 4, 128, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
+                                                  M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p,
+                                                  M.leaf_dblk.p, M.dense.p, Xf, Y, ldy, nr);
+    HM_LAUNCH_CHECK();
+  }
+  return HM_OK;
+}
+
+}  // namespace hm

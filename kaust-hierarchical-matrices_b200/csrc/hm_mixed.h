@@ -1,0 +1,100 @@
+// hm_mixed.h -- the mixed-precision (BF16 hi + lo) form of the H-matvec.
+//
+// Every cluster that owns low-rank factors gets one "panel": the factors of
+// all its blocks side by side (rows = the cluster's points, columns = the sum
+// of the blocks' ranks).  The projection of a whole block column is then one
+// dense panel^T X product, and the expansion of a block row one panel x T
+// product, so no block pays rank padding: the panel is padded once, to whole
+// 8-column tiles.  Columns whose BF16 rounding the tolerance cannot absorb
+// (the leading singular directions of each block) sit in the panel's first
+// tiles and carry a BF16 low part; the trailing ones are stored as BF16 only.
+//
+// Rows are padded per leaf to whole 32-row tiles ("global tiles"), so each
+// 32-row tile lies inside one leaf.  A tile of 32 rows x 8 columns is stored
+// in the order the mma.sync fragments want it: lane L of a warp loads one
+// 16-byte word and has its four fragment registers, 512 contiguous bytes per
+// warp load.  Two such orders exist per factor:
+//   P1 (phase 1, the factor is the B operand of X^T V, pairs along rows):
+//     lane (g,t) = {V[2t,2t+1][g], V[2t+8,2t+9][g], V[16+2t,17+2t][g], V[24+2t,25+2t][g]}
+//   P2 (phase 2, the factor is the A operand of U T, pairs along columns):
+//     lane (g,t) = {U[g][2t,2t+1], U[g+8][2t,2t+1], U[g+16][2t,2t+1], U[g+24][2t,2t+1]}
+// (g = lane / 4, t = lane % 4; each pair is bf16x2 with the lower index in the
+// low half).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "hm_internal.h"
+
+struct hm_hmatrix_s;
+
+namespace hm {
+
+struct MxPanel {
+  long long hi1, lo1, hi2, lo2;  // 512-byte tile offsets into MxPlan::store, [row tile][col tile]
+  long long s0;                  // first phase-1 output tile (nchunk x nct tiles)
+  long long t0;                  // first phase-2 input tile (nct tiles)
+  int nct, nctl;                 // 8-column tiles; the first nctl carry low parts
+  int tile0, nrt;                // first global row tile, row tiles
+  int nchunk;                    // row chunks of the projection
+  int r0;                        // first (tree-order) row of the cluster
+};
+
+struct MxUnit {  // phase-1 work item, one warp: up to 8 column tiles x up to 64 row tiles
+  int panel, ct0, nct, rt0, nrt, chunk;
+};
+
+struct MxDense {  // a dense block in P2 order, hi + lo, [row tile][col tile]
+  long long hi, lo;
+  int row_tile0, col_tile0;  // global row tiles of its row and column clusters
+  int nrt, nct;              // nct: 8-column tiles, a multiple of 4
+  int r0, c0, m, n;
+  const float* src;          // the FP32 block (m x n, column-major); read only while converting
+};
+
+struct MxPlan {
+  bool enabled = false;
+  DevBuf<uint4> store;  // all BF16 tiles
+  long long store_tiles = 0;
+  DevBuf<MxPanel> panels;
+  int num_panels = 0;
+  DevBuf<int> pan_of;      // heap-ordered cluster (2^l - 1 + a) -> panel or -1
+  DevBuf<MxUnit> units;
+  int num_units = 0;
+  DevBuf<int> tile_leaf;   // global row tile -> leaf
+  DevBuf<int> leaf_tile0;  // leaf -> first global row tile (num_leaves + 1)
+  int num_tiles = 0;
+  DevBuf<int2> tsrc;       // phase-2 column (8 * t0 + c) -> (source panel, source column) or (-1, -1)
+  long long s_tiles = 0, t_tiles = 0;
+  DevBuf<MxDense> dense;
+  int num_dense = 0;
+  DevBuf<int> leaf_dptr, leaf_dblk;  // dense blocks covering each leaf's rows
+  long long bytes_p1 = 0, bytes_p2 = 0;  // BF16 bytes of the factors (unpadded) and dense blocks
+  // scratch of one 16-column panel of right-hand sides, in floats
+  long long scratch_floats() const { return ((long long)num_tiles * 4 + s_tiles + t_tiles) * 128; }
+};
+
+struct MxPair {  // one stored low-rank pair (u rows, v columns) = fu fv^T, and its mirror
+  int level, r0, m, c0, n, k, khi;
+  const float* fu;  // m x k, column-major
+  const float* fv;  // n x k, column-major
+};
+
+struct MxDenseIn {
+  int r0, m, c0, n;
+  const float* D;  // m x n, column-major
+};
+
+// Builds the panels, converts the FP32 factors and dense blocks, and lays out
+// the phase-1 units and the column map of the projection.
+hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const std::vector<MxDenseIn>& dense,
+                      cudaStream_t s);
+
+// One panel of nr <= 16 right-hand sides in tree order; scratch holds
+// scratch_floats() floats.  e_mid (optional) is recorded between the
+// projection (split X, phase 1, column gather) and the expansion.
+hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, float* scratch,
+                          cudaStream_t s, cudaEvent_t e_mid);
+
+}  // namespace hm

@@ -59,6 +59,7 @@ class Stats(ctypes.Structure):
         ("factor_bytes", ctypes.c_longlong),
         ("dense_bytes", ctypes.c_longlong),
         ("num_unconverged", ctypes.c_longlong),
+        ("mixed_bytes", ctypes.c_longlong),
         ("build_seconds", ctypes.c_double),
     ]
 

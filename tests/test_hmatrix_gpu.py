@@ -22,7 +22,7 @@ def hm():
 
 
 def build(hm, n, d, b, kernel, ell, tol, max_rank, adm=1, eta=1.0, nugget=0.0, seed=1234, deriv=0,
-          points=None, sample_block=16):
+          points=None, sample_block=16, precision=0):
     import torch
 
     if points is None:
@@ -32,7 +32,7 @@ def build(hm, n, d, b, kernel, ell, tol, max_rank, adm=1, eta=1.0, nugget=0.0, s
     tree = hm.construct_kdtree(pts, n, d, b)
     st = hm.construct_hmatrix_structure(tree, adm, eta)
     H = hm.build_hmatrix(tree, st, pts, kernel=kernel, ell=ell, nugget=nugget, tol=tol, max_rank=max_rank,
-                         derivative=deriv, sample_block=sample_block)
+                         derivative=deriv, sample_block=sample_block, precision=precision)
     return pts.cpu().numpy(), tree, st, H
 
 
@@ -182,3 +182,65 @@ def test_rejects_bad_options(hm):
         hm.build_hmatrix(tree, st, pts, max_rank=200)
     with pytest.raises(hm.HMError):
         hm.build_hmatrix(tree, st, pts, sample_block=64)
+
+
+@pytest.mark.parametrize("n,d,b", [(20000, 3, 64), (13001, 2, 32)])
+def test_mixed_precision_matvec(hm, n, d, b):
+    """Precision form: factors stored as BF16 hi + lo (low parts only for the
+    leading columns the tolerance needs), products on BF16 tensor cores with
+    FP32 accumulation.  Its product error against the FP64 oracle stays within
+    the same bound as the FP32 form's, blocks still meet the tolerance, and the
+    adjoint equals the product bit for bit."""
+    import torch
+
+    kind, ell, nugget, tol = hm.K_MATERN32, 0.2, 1e-3, 1e-4
+    pts, tree, st, Hm = build(hm, n, d, b, kind, ell, tol, 128, nugget=nugget, seed=11, precision=hm.PREC_MIXED)
+    perm = tree.copy_out()["perm"]
+    s = Hm.stats()
+    assert s["num_unconverged"] == 0 and s["mixed_bytes"] > 0
+    check_blocks(Hm, pts, n, d, perm, kind, ell, nugget, tol, max_blocks=200)
+    rng = np.random.default_rng(9)
+    X = rng.standard_normal((n, 21))
+    Xd = torch.from_numpy(X.astype(np.float32)).cuda()
+    Y = Hm.matvec(Xd).cpu().numpy()
+    rows = rng.choice(n, 400, replace=False)
+    Yref = oracle.dense_rows_matvec(pts, n, d, perm, kind, ell, nugget, rows, X.T).T
+    err = np.linalg.norm(Y[rows] - Yref) / np.linalg.norm(Yref)
+    assert err < 1e-4, err
+    # per column, single right-hand side panels agree with the 16-wide panel
+    for c in (0, 20):
+        yc = Hm.matvec(Xd[:, c].contiguous()).cpu().numpy()[:, 0]
+        np.testing.assert_allclose(yc, Y[:, c], rtol=1e-5, atol=1e-5 * np.abs(Y[:, c]).max())
+    np.testing.assert_array_equal(Hm.matvec(Xd, trans=1).cpu().numpy(), Y)
+
+
+def _profile_bytes(hm, H, n):
+    import ctypes
+    import torch
+
+    L = hm.lib()
+    X = torch.randn((16, n), device="cuda", dtype=torch.float32)
+    Y = torch.empty_like(X)
+    mp, me = ctypes.c_float(), ctypes.c_float()
+    bp, be = ctypes.c_longlong(), ctypes.c_longlong()
+    hm._check(L.hm_hmatvec_profile(H.h, 16, hm._ptr(X), n, hm._ptr(Y), n, None, ctypes.byref(mp), ctypes.byref(me),
+                                   ctypes.byref(bp), ctypes.byref(be)))
+    return bp.value + be.value
+
+
+def test_mixed_moves_fewer_bytes_and_agrees_with_fp32(hm):
+    """The same cloud built in both forms: the mixed form's product agrees with
+    the FP32 form's to well inside the tolerance and streams fewer bytes."""
+    import torch
+
+    n, d, b = 30000, 3, 64
+    kind, ell, nugget, tol = hm.K_MATERN32, 0.2, 1e-3, 1e-4
+    pts, tree, st, Hf = build(hm, n, d, b, kind, ell, tol, 128, nugget=nugget, seed=21)
+    Hm = hm.build_hmatrix(tree, st, torch.from_numpy(pts).cuda(), kernel=kind, ell=ell, nugget=nugget, tol=tol,
+                          max_rank=128, precision=hm.PREC_MIXED)
+    X = torch.randn((n, 16), device="cuda", dtype=torch.float32)
+    Yf = Hf.matvec(X)
+    Ym = Hm.matvec(X)
+    rel = (torch.linalg.norm(Ym - Yf) / torch.linalg.norm(Yf)).item()
+    assert rel < 1e-4, rel
+    assert _profile_bytes(hm, Hm, n) < 0.8 * _profile_bytes(hm, Hf, n)
