@@ -364,6 +364,278 @@ __global__ void k_omega(float* om, int rows, int bs, uint32_t seed, int round) {
 }
 
 // ---------------------------------------------------------------------------
+// k_kmm_fast: the tensor-core sketch product specialised on the dimension
+// (1-3), the kernel and its derivative.  Coordinates are pre-scaled so that
+// each entry costs one hardware square root and one hardware exp2 (PTX
+// sqrt.approx / ex2.approx, both within a few ulp of FP32), the row
+// coordinates stay in registers, and the right-hand operand (the Gaussian
+// table in sampling mode, the basis Q in projection mode) is read as
+// prepacked BF16 pairs straight from L1/L2 instead of being restaged per chunk.
+// ---------------------------------------------------------------------------
+constexpr int kCC = 128;  // columns per coordinate chunk
+
+struct KmmFastArgs {
+  const Prob* probs;
+  ProbState* st;
+  const int2* items;
+  const float* pts;
+  int npts;
+  float scale;   // coordinate scale (see kval)
+  float dscale;  // derivative factor
+  int deriv;     // entries of dK/dl instead of K
+  int bs, round;
+  const uint32_t* om2;      // sampling: Gaussian pairs [jp][bs8]
+  int ld_om;                // bs8
+  const uint32_t* qh;       // projection: Q pairs [jp][kpad8], hi and lo, per problem
+  const uint32_t* ql;
+  const long long* qpoff;   // per problem (batch index), words
+  float* ws;
+};
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+constexpr float kLn2f = 0.6931471805599453f;
+
+// r2: squared distance of the scaled coordinates.
+//   KIND 0 (exp):    scale = log2(e)/l,         a = r log2(e)/l,  K = 2^-a
+//   KIND 1 (Matern): scale = sqrt(3) log2(e)/l,  K = (1 + a ln2) 2^-a
+//   KIND 2 (Gauss):  scale = sqrt(log2(e)/2)/l,  K = 2^-r2
+// derivatives dK/dl: exp a ln2 K / l, Matern (a ln2)^2 2^-a / l,
+// Gauss K q / l with q = r^2/l^2 = 2 ln2 r2.
+template <int KIND, bool DERIV>
+__device__ __forceinline__ float kval(float r2, float dscale) {
+  if (KIND == 2) {
+    const float v = ex2_approx(-r2);
+    return DERIV ? v * r2 * dscale : v;
+  }
+  const float a = sqrt_approx(r2);
+  const float e = ex2_approx(-a);
+  if (KIND == 1) {
+    const float al = a * kLn2f;
+    return DERIV ? al * al * e * dscale : fmaf(a, kLn2f, 1.0f) * e;
+  }
+  return DERIV ? a * e * dscale : e;
+}
+
+template <int D, int KIND, int MODE, int NT>
+__global__ void __launch_bounds__(128) k_kmm_fast(KmmFastArgs a) {
+  __shared__ float colc[D][kCC];
+  __shared__ double red[4];
+  const int2 it = a.items[blockIdx.x];
+  const Prob P = a.probs[it.x];
+  const ProbState S = a.st[it.x];
+  if (MODE == 0 && !S.active) return;
+  const int s = MODE == 0 ? a.bs : S.k;
+  if (s <= 0) return;
+  const int mr = MODE ? P.n : P.m;
+  const int nc = MODE ? P.m : P.n;
+  const int rbase = MODE ? P.c0 : P.r0;
+  const int cbase = MODE ? P.r0 : P.c0;
+  float* out = a.ws + (MODE ? P.boff : P.yoff);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int ra = it.y * kTR + warp * 16 + g, rb = ra + 8;
+  const bool ra_ok = ra < mr, rb_ok = rb < mr;
+  const bool deriv = a.deriv != 0;
+  float rca[D], rcb[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    rca[k] = ra_ok ? a.pts[(size_t)k * a.npts + rbase + ra] * a.scale : 0.f;
+    rcb[k] = rb_ok ? a.pts[(size_t)k * a.npts + rbase + rb] * a.scale : 0.f;
+  }
+  const int ntiles = min(NT, (s + 7) >> 3);
+  const uint32_t* Bh = MODE ? a.qh + a.qpoff[it.x] : a.om2;
+  const uint32_t* Bl = MODE ? a.ql + a.qpoff[it.x] : nullptr;
+  const size_t ldb = MODE ? (size_t)((s + 7) & ~7) : (size_t)a.ld_om;
+  float acc[NT][4];
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+  float nrm = 0.f;
+  const bool want_norm = MODE == 0 && a.round == 0;
+  // B fragments of k-step kg (16 columns): rows (8 kg + t) and (8 kg + t + 4) of the pair table
+  uint32_t bh[NT][2], bl[NT][2];
+  auto load_b = [&](int kg) {
+    const size_t w = (size_t)(8 * kg + t) * ldb + g;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      if (nt < ntiles) {
+        bh[nt][0] = __ldg(Bh + w + nt * 8);
+        bh[nt][1] = __ldg(Bh + w + 4 * ldb + nt * 8);
+        if (MODE == 1) {
+          bl[nt][0] = __ldg(Bl + w + nt * 8);
+          bl[nt][1] = __ldg(Bl + w + 4 * ldb + nt * 8);
+        }
+      }
+    }
+  };
+  const int nks = (nc + 15) >> 4;
+  load_b(0);
+  for (int kg = 0; kg < nks; ++kg) {
+    const int c0 = (kg * 16) / kCC * kCC;
+    if (kg * 16 == c0) {  // first k-step of a coordinate chunk
+      __syncthreads();
+      for (int e = threadIdx.x; e < D * kCC; e += blockDim.x) {
+        const int k = e / kCC, jj = e % kCC;
+        colc[k][jj] = c0 + jj < nc ? a.pts[(size_t)k * a.npts + cbase + c0 + jj] * a.scale : 0.f;
+      }
+      __syncthreads();
+    }
+    uint32_t ch[NT][2], cl[NT][2];
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      ch[nt][0] = bh[nt][0];
+      ch[nt][1] = bh[nt][1];
+      if (MODE == 1) {
+        cl[nt][0] = bl[nt][0];
+        cl[nt][1] = bl[nt][1];
+      }
+    }
+    if (kg + 1 < nks) load_b(kg + 1);  // in flight while this k-step's entries are generated
+    const int cb = kg * 16 - c0 + 2 * t;  // chunk columns cb, cb+1, cb+8, cb+9
+    float e[8];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = cb + (q & 1) + ((q >> 1) << 3);
+      const bool cok = c0 + c < nc;
+      float r2a = 0.f, r2b = 0.f;
+#pragma unroll
+      for (int k = 0; k < D; ++k) {
+        const float cc = colc[k][c];
+        const float da = rca[k] - cc, db = rcb[k] - cc;
+        r2a = fmaf(da, da, r2a);
+        r2b = fmaf(db, db, r2b);
+      }
+      const float va = deriv ? kval<KIND, true>(r2a, a.dscale) : kval<KIND, false>(r2a, a.dscale);
+      const float vb = deriv ? kval<KIND, true>(r2b, a.dscale) : kval<KIND, false>(r2b, a.dscale);
+      e[q] = (ra_ok && cok) ? va : 0.f;
+      e[4 + q] = (rb_ok && cok) ? vb : 0.f;
+    }
+    if (want_norm) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) nrm = fmaf(e[q], e[q], nrm);
+    }
+    uint32_t ah[4], al[4];
+    split_bf16x2(e[0], e[1], ah[0], al[0]);  // row g, cols cb, cb+1
+    split_bf16x2(e[4], e[5], ah[1], al[1]);  // row g+8
+    split_bf16x2(e[2], e[3], ah[2], al[2]);  // row g, cols cb+8, cb+9
+    split_bf16x2(e[6], e[7], ah[3], al[3]);  // row g+8
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      if (nt < ntiles) {
+        float d[4] = {0.f, 0.f, 0.f, 0.f};
+        if (MODE == 1) mma_bf16(d, ah[0], ah[1], ah[2], ah[3], cl[nt][0], cl[nt][1]);
+        mma_bf16(d, al[0], al[1], al[2], al[3], ch[nt][0], ch[nt][1]);
+        mma_bf16(d, ah[0], ah[1], ah[2], ah[3], ch[nt][0], ch[nt][1]);
+        add4(acc[nt], d);
+      }
+    }
+  }
+  const int ld = mr;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+    if (nt < ntiles) {
+      const int c = nt * 8 + 2 * t;
+      if (ra_ok) {
+        if (c < s) out[(size_t)c * ld + ra] = acc[nt][0];
+        if (c + 1 < s) out[(size_t)(c + 1) * ld + ra] = acc[nt][1];
+      }
+      if (rb_ok) {
+        if (c < s) out[(size_t)c * ld + rb] = acc[nt][2];
+        if (c + 1 < s) out[(size_t)(c + 1) * ld + rb] = acc[nt][3];
+      }
+    }
+  }
+  if (want_norm) {
+    double dn = nrm;
+    for (int o = 16; o > 0; o >>= 1) dn += __shfl_xor_sync(0xffffffffu, dn, o);
+    if (lane == 0) red[warp] = dn;
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(&a.st[it.x].normA2, red[0] + red[1] + red[2] + red[3]);
+  }
+}
+
+// Gaussian table of one sampling round in BF16 pairs: om2[jp][c] =
+// {W[2jp][c], W[2jp+1][c]} with W[j][c] the BF16-rounded N(0,1) value of
+// k_omega (columns c >= bs are zero).
+__global__ void k_omega_pack(uint32_t* om2, int rows2, int bs, int bs8, uint32_t seed, int round) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)rows2 * bs8;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int jp = (int)(e / bs8), c = (int)(e % bs8);
+    float x0 = 0.f, x1 = 0.f;
+    if (c < bs) {
+      x0 = gauss_at(seed, 0x51ed270bu + round, (uint32_t)(2 * jp), (uint32_t)c);
+      x1 = gauss_at(seed, 0x51ed270bu + round, (uint32_t)(2 * jp + 1), (uint32_t)c);
+    }
+    om2[e] = pack_bf16(x0, x1);
+  }
+}
+
+// Q (m x k, column-major, ld m) of each problem -> BF16 pairs along rows,
+// hi and lo: word (jp, c) = {Q[2jp][c], Q[2jp+1][c]}, jp < mpad/2, c < kpad8.
+__global__ void k_pack_q(const Prob* probs, const ProbState* st, const float* ws, const long long* qpoff,
+                         uint32_t* qh, uint32_t* ql) {
+  const Prob P = probs[blockIdx.x];
+  const int k = st[blockIdx.x].k;
+  if (k <= 0) return;
+  const int kp = (k + 7) & ~7;
+  const int rows2 = (P.m + kCC - 1) / kCC * (kCC / 2);
+  const float* Q = ws + P.qoff;
+  uint32_t* h = qh + qpoff[blockIdx.x];
+  uint32_t* l = ql + qpoff[blockIdx.x];
+  for (int e = threadIdx.x; e < rows2 * kp; e += blockDim.x) {
+    const int jp = e / kp, c = e % kp;
+    const int i0 = 2 * jp;
+    const float x0 = (c < k && i0 < P.m) ? Q[(size_t)c * P.m + i0] : 0.f;
+    const float x1 = (c < k && i0 + 1 < P.m) ? Q[(size_t)c * P.m + i0 + 1] : 0.f;
+    split_bf16x2(x0, x1, h[e], l[e]);
+  }
+}
+
+// nt: right-hand column tiles the launch must cover (sample block / 8, or
+// the largest basis of the batch / 8)
+template <int D, int KIND>
+void launch_kmm_fast3(int mode, int nt, unsigned grid, cudaStream_t s, const KmmFastArgs& a) {
+  if (mode == 0) {
+    if (nt <= 2)
+      k_kmm_fast<D, KIND, 0, 2><<<grid, 128, 0, s>>>(a);
+    else
+      k_kmm_fast<D, KIND, 0, kMaxBs / 8><<<grid, 128, 0, s>>>(a);
+  } else {
+    if (nt <= 4)
+      k_kmm_fast<D, KIND, 1, 4><<<grid, 128, 0, s>>>(a);
+    else if (nt <= 8)
+      k_kmm_fast<D, KIND, 1, 8><<<grid, 128, 0, s>>>(a);
+    else
+      k_kmm_fast<D, KIND, 1, kMaxCols / 8><<<grid, 128, 0, s>>>(a);
+  }
+}
+template <int D>
+void launch_kmm_fast2(int kind, int mode, int nt, unsigned grid, cudaStream_t s, const KmmFastArgs& a) {
+  if (kind == HM_KERNEL_GAUSS)
+    launch_kmm_fast3<D, 2>(mode, nt, grid, s, a);
+  else if (kind == HM_KERNEL_MATERN32)
+    launch_kmm_fast3<D, 1>(mode, nt, grid, s, a);
+  else
+    launch_kmm_fast3<D, 0>(mode, nt, grid, s, a);
+}
+void launch_kmm_fast(int d, int kind, int mode, int nt, unsigned grid, cudaStream_t s, const KmmFastArgs& a) {
+  if (d == 1)
+    launch_kmm_fast2<1>(kind, mode, nt, grid, s, a);
+  else if (d == 2)
+    launch_kmm_fast2<2>(kind, mode, nt, grid, s, a);
+  else
+    launch_kmm_fast2<3>(kind, mode, nt, grid, s, a);
+}
+
+// ---------------------------------------------------------------------------
 // per-block orthogonalisation of the new sample
 // ---------------------------------------------------------------------------
 template <typename W>
@@ -962,6 +1234,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   const std::vector<int>& lo = t->h_offsets;
   auto coff = [&](int level, int c) { return lo[(size_t)c << (depth - level)]; };
 
+  PhaseTrace tr("build");
   // ---- the problems: stored pairs (row cluster v > column cluster u) ------
   std::vector<uint32_t> tiles(std::max<long long>(s->start[depth], 1));
   if (s->start[depth] > 0)
@@ -986,6 +1259,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   }
   const long long nprob = (long long)probs.size();
 
+  tr.mark("problems", stream);
   // ---- batches bounded by the workspace budget -----------------------------
   size_t freeb = 0, totb = 0;
   HM_CUDA(cudaMemGetInfo(&freeb, &totb));
@@ -1010,17 +1284,36 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
     const size_t budget_elems = budget_bytes / sizeof(W);
     HM_CUDA(cudaFuncSetAttribute(k_kmm<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kmm_smem<W>()));
     HM_CUDA(cudaFuncSetAttribute(k_orth<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)orth_smem<W>()));
-    while (pstart < nprob) {
-      // greedy batch
-      long long pend = pstart;
+    // The specialised sketch kernels draw a double-width first sample (the
+    // generation of the kernel block, not its product with the sample, is
+    // the cost of a pass, so blocks of rank bs..2 bs finish a pass earlier).
+    constexpr bool kTensorW = std::is_same<W, float>::value;
+    const int bs_first = (kTensorW && t->d <= 3) ? std::min(2 * bs, kMaxBs) : bs;
+    // greedy batches under the workspace budget; one workspace for all of them
+    std::vector<long long> batch_end;
+    size_t ws_max = 1;
+    for (long long ps = pstart; ps < nprob;) {
+      long long pe = ps;
       size_t wsz = 0;
-      while (pend < nprob) {
-        const Prob& P = probs[pend];
-        size_t need = (size_t)P.m * (P.kmax + bs) + (size_t)P.m * bs + (size_t)P.n * (P.kmax + bs);
-        if (pend > pstart && wsz + need > budget_elems) break;
+      while (pe < nprob) {
+        const Prob& P = probs[pe];
+        size_t need = (size_t)P.m * (P.kmax + bs_first) + (size_t)P.m * bs_first + (size_t)P.n * (P.kmax + bs_first);
+        if (pe > ps && wsz + need > budget_elems) break;
         wsz += need;
-        ++pend;
+        ++pe;
       }
+      batch_end.push_back(pe);
+      ws_max = std::max(ws_max, wsz);
+      ps = pe;
+    }
+    DevBuf<W> ws;
+    {
+      hm_status st0 = ws.alloc(ws_max);
+      if (st0) return st0;
+    }
+    size_t bi = 0;
+    while (pstart < nprob) {
+      const long long pend = batch_end[bi++];
       const int nb = (int)(pend - pstart);
       std::vector<Prob> bp(probs.begin() + pstart, probs.begin() + pend);
       size_t off = 0;
@@ -1028,21 +1321,20 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       for (int i = 0; i < nb; ++i) {
         Prob& P = bp[i];
         P.qoff = (long long)off;
-        off += (size_t)P.m * (P.kmax + bs);
+        off += (size_t)P.m * (P.kmax + bs_first);
         P.yoff = (long long)off;
-        off += (size_t)P.m * bs;
+        off += (size_t)P.m * bs_first;
         P.boff = (long long)off;
-        off += (size_t)P.n * (P.kmax + bs);
+        off += (size_t)P.n * (P.kmax + bs_first);
         for (int tt = 0; tt * kTR < P.m; ++tt) items_rows.push_back(make_int2(i, tt));
         for (int tt = 0; tt * kTR < P.n; ++tt) items_cols.push_back(make_int2(i, tt));
       }
-      DevBuf<W> ws;
       DevBuf<Prob> dprobs;
       DevBuf<ProbState> dst;
       DevBuf<int2> drows, dcols;
       hm_status st;
-      if ((st = ws.alloc(std::max<size_t>(off, 1))) || (st = dprobs.alloc(nb)) || (st = dst.alloc(nb)) ||
-          (st = drows.alloc(items_rows.size())) || (st = dcols.alloc(items_cols.size())))
+      if ((st = dprobs.alloc_async(nb, stream)) || (st = dst.alloc_async(nb, stream)) ||
+          (st = drows.alloc_async(items_rows.size(), stream)) || (st = dcols.alloc_async(items_cols.size(), stream)))
         return st;
       std::vector<ProbState> hst(nb);
       for (auto& x : hst) {
@@ -1076,6 +1368,41 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       constexpr bool kTensor = std::is_same<W, float>::value;
       KmmTcArgs kt;
       DevBuf<float> omega;
+      // specialised sketch kernels for d <= 3
+      const bool fast = kTensor && t->d <= 3;
+      KmmFastArgs kf{};
+      DevBuf<uint32_t> om2;
+      int bs0 = bs_first;  // first round's sample width
+      for (const Prob& P : bp)
+        if (P.kmax < bs0) bs0 = bs;
+      const int bs8 = (bs0 + 7) & ~7;
+      int om_rows2 = 0;
+      if (fast) {
+        int max_n = 1;
+        for (const Prob& P : bp) max_n = std::max(max_n, P.n);
+        om_rows2 = (max_n + kCC - 1) / kCC * (kCC / 2);
+        if ((st = om2.alloc_async((size_t)om_rows2 * bs8, stream))) return st;
+        const double il = 1.0 / opt.ell, log2e = 1.4426950408889634, ln2 = 0.6931471805599453;
+        double sc = log2e * il, dsc = ln2 * il;
+        if (opt.kernel == HM_KERNEL_MATERN32) {
+          sc = std::sqrt(3.0) * log2e * il;
+          dsc = il;
+        } else if (opt.kernel == HM_KERNEL_GAUSS) {
+          sc = std::sqrt(0.5 * log2e) * il;
+          dsc = 2.0 * ln2 * il;
+        }
+        kf.probs = dprobs.p;
+        kf.st = dst.p;
+        kf.pts = t->pts_tree_f.p;
+        kf.npts = t->n;
+        kf.scale = (float)sc;
+        kf.dscale = (float)dsc;
+        kf.deriv = opt.derivative != 0;
+        kf.bs = bs;
+        kf.om2 = om2.p;
+        kf.ld_om = bs8;
+        kf.ws = reinterpret_cast<float*>(ws.p);
+      }
       if constexpr (kTensor) {
         int max_n = 1;
         for (const Prob& P : bp) max_n = std::max(max_n, P.n);
@@ -1091,9 +1418,19 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
         kt.ws = reinterpret_cast<float*>(ws.p);
         kt.omega_rows = max_n;
       }
+      tr.mark("batch setup", stream, nb);
       const int max_rounds = kMaxCols / bs + 2;
       for (int round = 0; round < max_rounds; ++round) {
-        if constexpr (kTensor) {
+        if (fast) {
+          const int rbs = round == 0 ? bs0 : bs;
+          k_omega_pack<<<592, 256, 0, stream>>>(om2.p, om_rows2, rbs, bs8, ka.seed, round);
+          HM_LAUNCH_CHECK();
+          kf.round = round;
+          kf.bs = rbs;
+          kf.items = drows.p;
+          oa.bs = rbs;
+          launch_kmm_fast(t->d, opt.kernel, 0, (rbs + 7) / 8, (unsigned)items_rows.size(), stream, kf);
+        } else if constexpr (kTensor) {
           k_omega<<<592, 256, 0, stream>>>(omega.p, kt.omega_rows, bs, ka.seed, round);
           HM_LAUNCH_CHECK();
           kt.mode = 0;
@@ -1116,8 +1453,51 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
         for (auto& x : hst) any |= x.active != 0;
         if (!any) break;
       }
+      tr.mark("sample rounds", stream, nb);
       // B = A^T Q
-      if constexpr (kTensor) {
+      DevBuf<uint32_t> qh, ql;
+      DevBuf<long long> dqpoff;
+      DevBuf<int2> dcls;
+      if (fast) {
+        std::vector<long long> qpoff(nb);
+        size_t qw = 0;
+        for (int i = 0; i < nb; ++i) {
+          qpoff[i] = (long long)qw;
+          if (hst[i].k > 0) qw += (size_t)(bp[i].m + kCC - 1) / kCC * (kCC / 2) * (size_t)((hst[i].k + 7) & ~7);
+        }
+        if ((st = qh.alloc_async(std::max<size_t>(qw, 1), stream)) ||
+            (st = ql.alloc_async(std::max<size_t>(qw, 1), stream)) || (st = dqpoff.alloc_async(nb, stream)))
+          return st;
+        HM_CUDA(cudaMemcpyAsync(dqpoff.p, qpoff.data(), sizeof(long long) * nb, cudaMemcpyHostToDevice, stream));
+        k_pack_q<<<nb, 256, 0, stream>>>(dprobs.p, dst.p, reinterpret_cast<const float*>(ws.p), dqpoff.p, qh.p,
+                                         ql.p);
+        HM_LAUNCH_CHECK();
+        kf.qh = qh.p;
+        kf.ql = ql.p;
+        kf.qpoff = dqpoff.p;
+        // one launch per basis-width class, so the narrow (most) blocks run
+        // with few accumulator registers
+        std::vector<int2> cls[3];
+        for (const int2& ic : items_cols) {
+          const int kk = hst[ic.x].k;
+          if (kk <= 0) continue;
+          cls[kk <= 32 ? 0 : (kk <= 64 ? 1 : 2)].push_back(ic);
+        }
+        const int cls_nt[3] = {4, 8, kMaxCols / 8};
+        size_t ncls = 0;
+        for (auto& c : cls) ncls += c.size();
+        if ((st = dcls.alloc_async(std::max<size_t>(ncls, 1), stream))) return st;
+        size_t o = 0;
+        for (int c = 0; c < 3; ++c) {
+          if (cls[c].empty()) continue;
+          HM_CUDA(cudaMemcpyAsync(dcls.p + o, cls[c].data(), sizeof(int2) * cls[c].size(), cudaMemcpyHostToDevice,
+                                  stream));
+          kf.items = dcls.p + o;
+          launch_kmm_fast(t->d, opt.kernel, 1, cls_nt[c], (unsigned)cls[c].size(), stream, kf);
+          HM_LAUNCH_CHECK();
+          o += cls[c].size();
+        }
+      } else if constexpr (kTensor) {
         kt.mode = 1;
         kt.items = dcols.p;
         k_kmm_tc<<<(unsigned)items_cols.size(), 128, 0, stream>>>(kt);
@@ -1128,6 +1508,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       }
       HM_LAUNCH_CHECK();
 
+      tr.mark("projection", stream, nb);
       // ---- truncation: Gram of B, Jacobi eigen, truncated rank -------------
       HM_CUDA(cudaMemcpyAsync(hst.data(), dst.p, sizeof(ProbState) * nb, cudaMemcpyDeviceToHost, stream));
       HM_CUDA(cudaStreamSynchronize(stream));
@@ -1161,6 +1542,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       HM_CUDA(cudaMemcpyAsync(hst.data(), dst.p, sizeof(ProbState) * nb, cudaMemcpyDeviceToHost, stream));
       HM_CUDA(cudaStreamSynchronize(stream));
 
+      tr.mark("truncation", stream, nb);
       // ---- results: low rank where converged, dense otherwise ---------------
       std::vector<long long> du(nb, -1), dv(nb, -1);
       std::vector<DenseItem> dens;
@@ -1242,6 +1624,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
           dense_bytes += 8ll * bp[i].m * bp[i].n;
         }
       }
+      tr.mark("factors", stream, nb);
       h->storage.push_back(std::move(chunk));
       pstart = pend;
     }
@@ -1288,6 +1671,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
     h->storage.push_back(std::move(chunk));
   }
 
+  tr.mark("diagonal leaves", stream);
   // ---- block lists (both orientations) --------------------------------------
   for (long long i = 0; i < nprob; ++i) {
     const Prob& P = probs[i];
@@ -1317,6 +1701,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       h->h_dense.push_back(dt);
     }
   }
+  tr.mark("block lists", stream);
   // ---- mixed precision form -------------------------------------------------
   if (opt.precision == HM_PREC_MIXED) {
     std::vector<MxPair> mp;
@@ -1338,8 +1723,10 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   h->stats.factor_bytes = factor_bytes;
   h->stats.dense_bytes = dense_bytes;
   h->stats.num_unconverged = unconverged;
+  tr.mark("mixed panels", stream);
   hm_status st = matvec_plan_build(h, 16, stream);
   if (st) return cleanup(st);
+  tr.mark("matvec plan", stream);
   HM_CUDA(cudaEventRecord(ev1, stream));
   HM_CUDA(cudaEventSynchronize(ev1));
   float ms = 0;

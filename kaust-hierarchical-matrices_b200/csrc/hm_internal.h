@@ -4,6 +4,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -31,6 +34,32 @@ hm_status cuda_fail(cudaError_t e, const char* what, const char* file, int line)
   } while (0)
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ---- phase trace --------------------------------------------------------------
+// With HM_TRACE=1 in the environment, a build prints the wall-clock time of
+// each phase to stderr (the stream is synchronised at every mark, so device
+// work is charged to the phase that launched it).  Off, a mark costs nothing.
+struct PhaseTrace {
+  bool on = false;
+  const char* what = "";
+  std::chrono::steady_clock::time_point last;
+  explicit PhaseTrace(const char* w) : what(w) {
+    const char* e = std::getenv("HM_TRACE");
+    on = e != nullptr && e[0] != '\0' && e[0] != '0';
+    last = std::chrono::steady_clock::now();
+  }
+  void mark(const char* phase, cudaStream_t s, long long arg = -1) {
+    if (!on) return;
+    cudaStreamSynchronize(s);
+    const auto now = std::chrono::steady_clock::now();
+    const double ms = std::chrono::duration<double, std::milli>(now - last).count();
+    if (arg >= 0)
+      std::fprintf(stderr, "[hm trace] %s %-24s %5lld %10.3f ms\n", what, phase, arg, ms);
+    else
+      std::fprintf(stderr, "[hm trace] %s %-24s       %10.3f ms\n", what, phase, ms);
+    last = now;
+  }
+};
 
 // ---- device buffer RAII -----------------------------------------------------
 // Long-lived buffers use cudaMalloc; temporaries of a build step pass a stream
