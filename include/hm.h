@@ -216,6 +216,16 @@ HM_API hm_status hm_hmatvec_profile(hm_hmatrix h, int nrhs, const float* X, int 
                                     void* stream, float* ms_project, float* ms_expand,
                                     long long* bytes_project, long long* bytes_expand);
 
+/* Per-kernel device times of one product (nrhs <= 16, X and Y in tree order):
+ * CUDA events on `stream` after each kernel, synchronised before return.
+ * Fills up to `cap` entries of names (static strings), ms and algorithmic
+ * bytes (what the kernel must read and write at least); *count receives the
+ * number of kernels the product launched.  For measurement only; no
+ * counterpart in the reference. */
+HM_API hm_status hm_hmatvec_kernels(hm_hmatrix h, int nrhs, const float* X, int ldx, float* Y, int ldy,
+                                    void* stream, int cap, const char** names, float* ms, long long* bytes,
+                                    int* count);
+
 /* Block list as the matvec sees it (both orientations of each stored pair),
  * the counterpart of the reference's HMatrixLevel (src/HMatrix.cuh:9-18).
  * Any pointer may be NULL.  lowrank: *num_lowrank rows of 6 ints

@@ -8,6 +8,23 @@
 
 namespace hm {
 
+// Events recorded after each kernel of one product, for per-kernel device
+// times (profiling entry points only; the hot path passes nullptr).
+struct KernelMarks {
+  static constexpr int kMax = 8;
+  cudaEvent_t ev[kMax + 1];
+  const char* name[kMax];
+  long long bytes[kMax];  // algorithmic bytes of each kernel
+  int n = 0;
+  void mark(const char* nm, long long b, cudaStream_t s) {
+    if (n >= kMax) return;
+    name[n] = nm;
+    bytes[n] = b;
+    cudaEventRecord(ev[n + 1], s);
+    ++n;
+  }
+};
+
 // One block of the matrix as the matvec sees it (both orientations of a stored
 // pair appear, the mirror one with U and V exchanged).
 struct LRBlock {
@@ -57,6 +74,8 @@ struct MatvecPlan {
   int num_leaves = 0;
   int maxleaf = 1;
   DevBuf<float> Xp, Yp;      // permuted copies for original-order calls (n * nrhs_cap)
+  long long bytes_p1 = 0, bytes_p2 = 0;  // FP32 factor bytes read by each phase (+ dense in phase 2)
+  long long multi_t_floats = 0;          // projections written by the chunk reduction
 };
 
 }  // namespace hm

@@ -274,24 +274,26 @@ __global__ void k_scatter_rows(const float* Yp, const int* perm, int n, int nrhs
 // One panel of nr <= 16 right-hand sides (X, Y in tree order); T: projection
 // scratch (16 x kpad per block, then the chunk partials).
 hm_status run_panel(hm_hmatrix h, int nr, const float* X, int ldx, float* Y, int ldy, float* T, cudaStream_t s,
-                    cudaEvent_t e_mid) {
-  if (h->mx.enabled) return mixed_run_panel(h, nr, X, ldx, Y, ldy, T, s, e_mid);
+                    KernelMarks* km) {
+  if (h->mx.enabled) return mixed_run_panel(h, nr, X, ldx, Y, ldy, T, s, km);
   MatvecPlan& P = h->plan;
   float* Tpart = T + P.t_floats;
   if (P.num_p1 > 0) {
     k_p1<<<(P.num_p1 + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, s>>>(P.p1.p, P.num_p1, P.lr.p, X,
                                                                                      ldx, nr, T, Tpart);
     HM_LAUNCH_CHECK();
+    if (km) km->mark("k_p1", P.bytes_p1 + 4ll * h->n * nr, s);
   }
   if (P.num_multi > 0) {
     k_reduce_multi<<<std::min(P.num_multi, 8192), 128, 0, s>>>(P.multi.p, P.num_multi, Tpart, T);
     HM_LAUNCH_CHECK();
+    if (km) km->mark("k_reduce_multi", 4ll * P.part_floats + 4ll * P.multi_t_floats, s);
   }
-  if (e_mid) HM_CUDA(cudaEventRecord(e_mid, s));
   k_p2<<<(P.num_groups + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, s>>>(
       P.groups.p, P.num_groups, h->tree->offsets.p, P.leaf_ptr.p, P.leaf_blk.p, P.lr.p, P.leaf_dptr.p,
       P.leaf_dblk.p, P.dense.p, T, X, ldx, nr, Y, ldy);
   HM_LAUNCH_CHECK();
+  if (km) km->mark("k_p2", P.bytes_p2 + 8ll * h->n * nr, s);
   return HM_OK;
 }
 
@@ -333,6 +335,13 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   P.num_p1 = (int)items.size();
   P.num_multi = (int)multi.size();
   P.part_floats = part;
+  P.bytes_p1 = P.bytes_p2 = P.multi_t_floats = 0;
+  for (const auto& b : h->h_lr) {
+    P.bytes_p1 += 4ll * b.n * b.k;
+    P.bytes_p2 += 4ll * b.m * b.k;
+  }
+  for (const auto& d : h->h_dense) P.bytes_p2 += 4ll * d.m * d.n;
+  for (const auto& mi : multi) P.multi_t_floats += 16ll * mi.kpad;
   // phase 2: leaf lists
   auto leaf_range = [&](int r0, int m, int& a, int& b) {
     a = (int)(std::lower_bound(lo.begin(), lo.end() - 1, r0) - lo.begin());
@@ -487,6 +496,20 @@ hm_status noalloc_scratch(float** out) {
 }  // namespace
 }  // namespace hm
 
+namespace hm {
+// One panel with an event after each kernel; synchronises.  The caller
+// destroys km->ev.
+hm_status timed_panel(hm_hmatrix h, int nr, const float* X, int ldx, float* Y, int ldy, cudaStream_t s,
+                      KernelMarks* km) {
+  for (auto& x : km->ev) HM_CUDA(cudaEventCreate(&x));
+  km->n = 0;
+  HM_CUDA(cudaEventRecord(km->ev[0], s));
+  HM_TRY(run_panel(h, nr, X, ldx, Y, ldy, h->plan.T.p, s, km));
+  HM_CUDA(cudaEventSynchronize(km->ev[km->n]));
+  return HM_OK;
+}
+}  // namespace hm
+
 // The product of hm_hmatvec (tree order) with its projection workspace taken
 // from the library's static scratch instead of the matrix's own buffer; no
 // allocation of any kind.
@@ -527,21 +550,40 @@ extern "C" hm_status hm_hmatvec_profile(hm_hmatrix h, int nrhs, const float* X, 
   if (nrhs < 1 || nrhs > 16 || !X || !Y || ldx < h->n || ldy < h->n)
     return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: need 1 <= nrhs <= 16 and valid vectors");
   cudaStream_t s = hm::as_stream(stream);
-  cudaEvent_t e[3];
-  for (auto& x : e) HM_CUDA(cudaEventCreate(&x));
-  HM_CUDA(cudaEventRecord(e[0], s));
-  HM_TRY(hm::run_panel(h, nrhs, X, ldx, Y, ldy, h->plan.T.p, s, e[1]));
-  HM_CUDA(cudaEventRecord(e[2], s));
-  HM_CUDA(cudaEventSynchronize(e[2]));
+  hm::KernelMarks km;
+  HM_TRY(hm::timed_panel(h, nrhs, X, ldx, Y, ldy, s, &km));
+  // projection: every kernel but the last; expansion: the last
   float a = 0, b = 0;
-  HM_CUDA(cudaEventElapsedTime(&a, e[0], e[1]));
-  HM_CUDA(cudaEventElapsedTime(&b, e[1], e[2]));
-  for (auto& x : e) cudaEventDestroy(x);
+  if (km.n > 0) {
+    HM_CUDA(cudaEventElapsedTime(&a, km.ev[0], km.ev[km.n - 1]));
+    HM_CUDA(cudaEventElapsedTime(&b, km.ev[km.n - 1], km.ev[km.n]));
+  }
+  for (auto& x : km.ev) cudaEventDestroy(x);
   if (ms_project) *ms_project = a;
   if (ms_expand) *ms_expand = b;
   long long bp = 0, be = 0;
   hm::matvec_bytes(h, nrhs, &bp, &be);
   if (bytes_project) *bytes_project = bp;
   if (bytes_expand) *bytes_expand = be;
+  return HM_OK;
+}
+
+extern "C" hm_status hm_hmatvec_kernels(hm_hmatrix h, int nrhs, const float* X, int ldx, float* Y, int ldy,
+                                        void* stream, int cap, const char** names, float* ms, long long* bytes,
+                                        int* count) {
+  if (!h) return hm::fail(HM_ERR_INVALID, "hm_hmatvec_kernels: null matrix");
+  if (nrhs < 1 || nrhs > 16 || !X || !Y || ldx < h->n || ldy < h->n || cap < 0)
+    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_kernels: need 1 <= nrhs <= 16 and valid vectors");
+  hm::KernelMarks km;
+  HM_TRY(hm::timed_panel(h, nrhs, X, ldx, Y, ldy, hm::as_stream(stream), &km));
+  for (int i = 0; i < km.n && i < cap; ++i) {
+    float t = 0;
+    cudaEventElapsedTime(&t, km.ev[i], km.ev[i + 1]);
+    if (names) names[i] = km.name[i];
+    if (ms) ms[i] = t;
+    if (bytes) bytes[i] = km.bytes[i];
+  }
+  if (count) *count = km.n;
+  for (auto& x : km.ev) cudaEventDestroy(x);
   return HM_OK;
 }

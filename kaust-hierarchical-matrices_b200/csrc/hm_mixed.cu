@@ -589,7 +589,7 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
 }
 
 hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, float* scratch,
-                          cudaStream_t s, cudaEvent_t e_mid) {
+                          cudaStream_t s, KernelMarks* km) {
   MxPlan& M = h->mx;
   uint4* Xf = reinterpret_cast<uint4*>(scratch);
   float* S = scratch + (size_t)M.num_tiles * 4 * 128;
@@ -599,22 +599,25 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
     k_mx_split_x<<<(M.num_tiles + 3) / 4, 128, 0, s>>>(X, ldx, nr, M.num_tiles, M.tile_leaf.p, M.leaf_tile0.p,
                                                        leaf_off, Xf);
     HM_LAUNCH_CHECK();
+    if (km) km->mark("k_mx_split_x", 4ll * h->n * nr + 4ll * h->n * 16, s);
   }
   if (M.num_units > 0) {
     k_mx_p1<<<(M.num_units + 3) / 4, 128, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf,
                                                   reinterpret_cast<float4*>(S));
     HM_LAUNCH_CHECK();
+    if (km) km->mark("k_mx_p1", M.bytes_p1 + 4ll * h->n * 16, s);
   }
   if (M.t_tiles > 0) {
     k_mx_gather<<<(unsigned)((M.t_tiles * 32 + 255) / 256), 256, 0, s>>>(M.tsrc.p, M.t_tiles, M.panels.p, S, T);
     HM_LAUNCH_CHECK();
+    if (km) km->mark("k_mx_gather", 2ll * h->stats.rank_sum * 16 * 4, s);
   }
-  if (e_mid) HM_CUDA(cudaEventRecord(e_mid, s));
   if (M.num_tiles > 0) {
     k_mx_p2<<<(M.num_tiles + 3) / 4, 128, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
                                                   M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p,
                                                   M.leaf_dblk.p, M.dense.p, Xf, Y, ldy, nr);
     HM_LAUNCH_CHECK();
+    if (km) km->mark("k_mx_p2", M.bytes_p2 + 4ll * h->n * 16 + 4ll * h->n * nr, s);
   }
   return HM_OK;
 }

@@ -91,10 +91,11 @@ struct MxDenseIn {
 hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const std::vector<MxDenseIn>& dense,
                       cudaStream_t s);
 
+struct KernelMarks;
+
 // One panel of nr <= 16 right-hand sides in tree order; scratch holds
-// scratch_floats() floats.  e_mid (optional) is recorded between the
-// projection (split X, phase 1, column gather) and the expansion.
+// scratch_floats() floats.  km (optional) receives an event after each kernel.
 hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, float* scratch,
-                          cudaStream_t s, cudaEvent_t e_mid);
+                          cudaStream_t s, KernelMarks* km);
 
 }  // namespace hm
