@@ -151,6 +151,8 @@ typedef struct {
   int precision;       /* hm_precision */
   int derivative;      /* 0: K, 1: dK/dl */
   unsigned long long seed;  /* seed of the Gaussian test matrices */
+  int diag_from_coords;     /* diagonal leaf blocks: 0 stored, 1 recomputed from the coordinates in
+                               every product, -1 (default) recomputed for derivative builds only */
 } hm_build_opts;
 
 /* Fills opts with the reference's settings: exp kernel, l = 0.2 if d == 3

@@ -1637,7 +1637,8 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
 
   // ---- diagonal leaves ------------------------------------------------------
   const int nleaf = 1 << depth;
-  {
+  h->diag_fly = opt.diag_from_coords > 0 || (opt.diag_from_coords < 0 && opt.derivative != 0);
+  if (!h->diag_fly) {
     std::vector<DenseItem> dens(nleaf);
     size_t tot = 0;
     for (int l = 0; l < nleaf; ++l) {
@@ -1754,6 +1755,7 @@ void hm_build_opts_default(int d, hm_build_opts* o) {
   o->precision = HM_PREC_FP32;
   o->derivative = 0;
   o->seed = 0;
+  o->diag_from_coords = -1;
 }
 
 hm_status hm_hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, const hm_build_opts* opts,

@@ -25,6 +25,11 @@ struct KernelMarks {
   }
 };
 
+// Y[leaf rows] += K(leaf, leaf) X[leaf rows] for every leaf, entries from the
+// coordinates (the diagonal blocks of a matrix built with diag_fly).
+hm_status diag_fly_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, cudaStream_t s,
+                         KernelMarks* km);
+
 // One block of the matrix as the matvec sees it (both orientations of a stored
 // pair appear, the mirror one with U and V exchanged).
 struct LRBlock {
@@ -90,6 +95,7 @@ struct hm_hmatrix_s {
   hm_hmatrix_stats stats{};
   hm::MatvecPlan plan;
   hm::MxPlan mx;                     // mixed precision form (panels of BF16 hi + lo tiles)
+  bool diag_fly = false;             // diagonal leaf blocks recomputed from the coordinates per product
   // host mirror of the block list (for export / tests)
   std::vector<hm::LRBlock> h_lr;
   std::vector<hm::DenseBlock> h_dense;

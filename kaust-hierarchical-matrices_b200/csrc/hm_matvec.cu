@@ -271,6 +271,57 @@ __global__ void k_scatter_rows(const float* Yp, const int* perm, int n, int nrhs
 }
 
 
+// Y[leaf] += K(leaf, leaf) X[leaf], one CTA per leaf, entries from the
+// tree-ordered FP32 coordinates exactly as the stored diagonal blocks are
+// generated (kernel_r2, plus the nugget on the diagonal unless dK/dl).
+constexpr int kFlyT = 64;
+__global__ void __launch_bounds__(kFlyT) k_diag_fly(const int* __restrict__ leaf_off, const float* __restrict__ pts,
+                                                    int npts, int d, KernelParams kp, const float* __restrict__ X,
+                                                    int ldx, int nr, float* __restrict__ Y, int ldy) {
+  __shared__ float cs[kMaxDim][kFlyT];
+  __shared__ float xs[16][kFlyT];
+  const int r0 = leaf_off[blockIdx.x];
+  const int m = leaf_off[blockIdx.x + 1] - r0;
+  for (int i0 = 0; i0 < m; i0 += kFlyT) {
+    const int i = i0 + threadIdx.x;
+    const bool iok = i < m;
+    float ci[kMaxDim];
+#pragma unroll
+    for (int k = 0; k < kMaxDim; ++k) ci[k] = (k < d && iok) ? pts[(size_t)k * npts + r0 + i] : 0.f;
+    float acc[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) acc[r] = 0.f;
+    for (int j0 = 0; j0 < m; j0 += kFlyT) {
+      __syncthreads();
+      const int j = j0 + threadIdx.x;
+      for (int k = 0; k < d; ++k) cs[k][threadIdx.x] = j < m ? pts[(size_t)k * npts + r0 + j] : 0.f;
+#pragma unroll
+      for (int r = 0; r < 16; ++r) xs[r][threadIdx.x] = (j < m && r < nr) ? X[(size_t)r * ldx + r0 + j] : 0.f;
+      __syncthreads();
+      const int jn = min(kFlyT, m - j0);
+      for (int jj = 0; jj < jn; ++jj) {
+        float r2 = 0.f;
+#pragma unroll
+        for (int k = 0; k < kMaxDim; ++k) {
+          if (k < d) {
+            const float df = ci[k] - cs[k][jj];
+            r2 = fmaf(df, df, r2);
+          }
+        }
+        float e = kernel_r2(kp, r2);
+        if (i == j0 + jj && !kp.deriv) e += kp.nugget;
+#pragma unroll
+        for (int r = 0; r < 16; ++r) acc[r] = fmaf(e, xs[r][jj], acc[r]);
+      }
+    }
+    if (iok) {
+#pragma unroll
+      for (int r = 0; r < 16; ++r)
+        if (r < nr) Y[(size_t)r * ldy + r0 + i] += acc[r];
+    }
+  }
+}
+
 // One panel of nr <= 16 right-hand sides (X, Y in tree order); T: projection
 // scratch (16 x kpad per block, then the chunk partials).
 hm_status run_panel(hm_hmatrix h, int nr, const float* X, int ldx, float* Y, int ldy, float* T, cudaStream_t s,
@@ -294,6 +345,7 @@ hm_status run_panel(hm_hmatrix h, int nr, const float* X, int ldx, float* Y, int
       P.leaf_dblk.p, P.dense.p, T, X, ldx, nr, Y, ldy);
   HM_LAUNCH_CHECK();
   if (km) km->mark("k_p2", P.bytes_p2 + 8ll * h->n * nr, s);
+  if (h->diag_fly) HM_TRY(diag_fly_panel(h, nr, X, ldx, Y, ldy, s, km));
   return HM_OK;
 }
 
@@ -497,6 +549,16 @@ hm_status noalloc_scratch(float** out) {
 }  // namespace hm
 
 namespace hm {
+hm_status diag_fly_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, cudaStream_t s,
+                         KernelMarks* km) {
+  const int nleaf = 1 << h->depth;
+  const hm_kdtree t = h->tree;
+  k_diag_fly<<<nleaf, kFlyT, 0, s>>>(t->offsets.p, t->pts_tree_f.p, t->n, t->d, h->kp, X, ldx, nr, Y, ldy);
+  HM_LAUNCH_CHECK();
+  if (km) km->mark("k_diag_fly", 4ll * h->n * nr * 3 + 4ll * h->n * h->d, s);
+  return HM_OK;
+}
+
 // One panel with an event after each kernel; synchronises.  The caller
 // destroys km->ev.
 hm_status timed_panel(hm_hmatrix h, int nr, const float* X, int ldx, float* Y, int ldy, cudaStream_t s,

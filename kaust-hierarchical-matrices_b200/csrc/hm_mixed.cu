@@ -619,6 +619,7 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_mx_p2", M.bytes_p2 + 4ll * h->n * 16 + 4ll * h->n * nr, s);
   }
+  if (h->diag_fly) HM_TRY(diag_fly_panel(h, nr, X, ldx, Y, ldy, s, km));
   return HM_OK;
 }
 

@@ -47,6 +47,7 @@ class BuildOpts(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("derivative", ctypes.c_int),
         ("seed", ctypes.c_ulonglong),
+        ("diag_from_coords", ctypes.c_int),
     ]
 
 
@@ -296,7 +297,8 @@ def default_opts(d):
 
 
 def build_hmatrix(tree, structure, points=None, kernel=K_EXP, ell=None, nugget=0.0, tol=1e-5, max_rank=64,
-                  leaf_max_rank=0, sample_block=16, precision=PREC_FP32, derivative=0, seed=0, stream=None):
+                  leaf_max_rank=0, sample_block=16, precision=PREC_FP32, derivative=0, seed=0, stream=None,
+                  diag_from_coords=-1):
     o = default_opts(tree.d)
     o.kernel = kernel
     if ell is not None:
@@ -309,6 +311,7 @@ def build_hmatrix(tree, structure, points=None, kernel=K_EXP, ell=None, nugget=0
     o.precision = precision
     o.derivative = derivative
     o.seed = seed
+    o.diag_from_coords = diag_from_coords
     h = ctypes.c_void_p()
     _check(lib().hm_hmatrix_build(tree.h, structure.h, _ptr(points) if points is not None else None,
                                   ctypes.byref(o), _stream(stream), ctypes.byref(h)))
