@@ -68,6 +68,7 @@ typedef enum {
 typedef struct hm_kdtree_s* hm_kdtree;
 typedef struct hm_structure_s* hm_structure;
 typedef struct hm_hmatrix_s* hm_hmatrix;
+typedef struct hm_batch_s* hm_batch;
 
 /* Message describing the last failure on this thread ("" if none). */
 HM_API const char* hm_last_error(void);
@@ -241,6 +242,38 @@ HM_API hm_status hm_hmatrix_blocks(hm_hmatrix h, long long* num_lowrank, long lo
 HM_API hm_status hm_hmatrix_block_factors(hm_hmatrix h, int i, float* U, float* V);
 
 HM_API void hm_hmatrix_free(hm_hmatrix h);
+
+/* --- Batches of independent clouds ------------------------------------------
+ * No counterpart in the reference (one cloud per run, src/main.cu:33-200).
+ * A batch joins C clouds (each with its own KD tree and block structure) as
+ * the subtrees of one forest, so that one build compresses the blocks of all
+ * clouds in the same batched launches and one product covers all clouds.
+ * Rows are the clouds' tree-order rows concatenated: cloud c owns rows
+ * [row_offsets[c], row_offsets[c+1]).  The trees and structures must outlive
+ * the batch; all clouds share the dimension and the admissibility rule, and
+ * the forest may be at most 16 levels deep (ceil(log2 C) + the deepest tree). */
+HM_API hm_status hm_batch_create(int nclouds, const hm_kdtree* trees, const hm_structure* structures, void* stream,
+                                 hm_batch* out);
+
+/* row_offsets: nclouds + 1 ints; any pointer may be NULL. */
+HM_API hm_status hm_batch_info(hm_batch b, int* nclouds, int* n_total, int* depth, int* row_offsets);
+
+/* Builds (or rebuilds) the batch's H-matrix with the given options. */
+HM_API hm_status hm_batch_build(hm_batch b, const hm_build_opts* opts, void* stream);
+
+/* The batch's H-matrix (owned by the batch): stats, blocks, hm_hmatvec. */
+HM_API hm_hmatrix hm_batch_hmatrix(hm_batch b);
+
+/* Y = H X over all clouds (X, Y: n_total x nrhs, column-major; tree order,
+ * or each cloud's original order when original_order != 0).  The first call
+ * for a given (X, Y, nrhs, ldx, ldy, original_order, stream) records the
+ * product's kernels into a CUDA graph; every call launches that graph, one
+ * launch for the whole batch.  `stream` must be a created stream (the legacy
+ * default stream cannot be recorded). */
+HM_API hm_status hm_batch_matvec(hm_batch b, int nrhs, const float* X, int ldx, float* Y, int ldy,
+                                 int original_order, void* stream);
+
+HM_API void hm_batch_free(hm_batch b);
 
 #ifdef __cplusplus
 }

@@ -98,6 +98,14 @@ def lib():
             L.hm_hmatrix_free.argtypes = [P]
             L.hm_hmatrix_blocks.argtypes = [P, P, P, P, P]
             L.hm_hmatrix_block_factors.argtypes = [P, I, P, P]
+            L.hm_hmatvec_kernels.argtypes = [P, I, P, I, P, I, P, I, P, P, P, P]
+            L.hm_batch_create.argtypes = [I, P, P, P, ctypes.POINTER(P)]
+            L.hm_batch_info.argtypes = [P, P, P, P, P]
+            L.hm_batch_build.argtypes = [P, ctypes.POINTER(BuildOpts), P]
+            L.hm_batch_hmatrix.argtypes = [P]
+            L.hm_batch_hmatrix.restype = P
+            L.hm_batch_matvec.argtypes = [P, I, P, I, P, I, I, P]
+            L.hm_batch_free.argtypes = [P]
         _lib = L
     return _lib
 
@@ -279,8 +287,65 @@ class HMatrix:
         return (U[: m * k].reshape(k, m).T.astype(np.float64), V[: n * k].reshape(k, n).T.astype(np.float64))
 
     def free(self):
-        if self.h:
+        if self.h and getattr(self, "owned", True):
             lib().hm_hmatrix_free(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Independent clouds joined as one forest (hm_batch_*): one build for all
+    clouds, one graph-launched product over the concatenated rows."""
+
+    def __init__(self, trees, structures, stream=None):
+        n = len(trees)
+        self.trees, self.structures = list(trees), list(structures)  # kept alive
+        val = lambda h: h.value if isinstance(h, ctypes.c_void_p) else h
+        th = (ctypes.c_void_p * n)(*[val(t.h) for t in trees])
+        sh = (ctypes.c_void_p * n)(*[val(s.h) for s in structures])
+        h = ctypes.c_void_p()
+        _check(lib().hm_batch_create(n, th, sh, _stream(stream), ctypes.byref(h)))
+        self.h = h
+        nc, nt, dep = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        offs = (ctypes.c_int * (n + 1))()
+        _check(lib().hm_batch_info(self.h, ctypes.byref(nc), ctypes.byref(nt), ctypes.byref(dep), offs))
+        self.nclouds, self.n, self.depth = nc.value, nt.value, dep.value
+        self.row_offsets = list(offs)
+
+    def build(self, kernel=K_EXP, ell=None, nugget=0.0, tol=1e-5, max_rank=64, leaf_max_rank=0, sample_block=16,
+              precision=PREC_FP32, derivative=0, seed=0, stream=None, diag_from_coords=-1):
+        o = default_opts(self.trees[0].d)
+        o.kernel, o.nugget, o.tol, o.max_rank = kernel, nugget, tol, max_rank
+        if ell is not None:
+            o.ell = ell
+        o.leaf_max_rank, o.sample_block, o.precision = leaf_max_rank, sample_block, precision
+        o.derivative, o.seed, o.diag_from_coords = derivative, seed, diag_from_coords
+        _check(lib().hm_batch_build(self.h, ctypes.byref(o), _stream(stream)))
+
+    def hmatrix(self):
+        """The batch's H-matrix (owned by the batch)."""
+        H = HMatrix(lib().hm_batch_hmatrix(self.h), self, None)
+        H.owned = False
+        return H
+
+    def matvec(self, X, Y, stream, original_order=False):
+        """Y = H X over all clouds through the recorded CUDA graph; X, Y float32
+        CUDA tensors (n_total, nrhs) with X.T, Y.T contiguous; stream: a
+        torch.cuda.Stream (not the legacy default stream)."""
+        Xc, Yc = X.t(), Y.t()
+        assert Xc.is_contiguous() and Yc.is_contiguous()
+        _check(lib().hm_batch_matvec(self.h, X.shape[1], _ptr(Xc), self.n, _ptr(Yc), self.n,
+                                     1 if original_order else 0, _stream(stream)))
+        return Y
+
+    def free(self):
+        if self.h:
+            lib().hm_batch_free(self.h)
             self.h = None
 
     def __del__(self):
