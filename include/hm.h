@@ -243,6 +243,18 @@ HM_API hm_status hm_hmatrix_block_factors(hm_hmatrix h, int i, float* U, float* 
 
 HM_API void hm_hmatrix_free(hm_hmatrix h);
 
+/* Schedule autotuner (no counterpart in the reference).  Times the product's
+ * schedule candidates on this matrix (nrhs columns, <= 16) and keeps the
+ * fastest: for the FP32 form the rows of V per phase-1 item, for the mixed
+ * form the phase-1 unit shape.  With cache_path set, the choice is appended
+ * to that text file under a key of the GPU and the matrix's shape, and a
+ * later call whose key is in the file applies the cached choice without
+ * timing (*from_cache = 1).  choice receives a description (may be NULL).
+ * Products recorded into graphs before the call must be recorded again
+ * (hm_batch_matvec does that by itself). */
+HM_API hm_status hm_autotune(hm_hmatrix h, int nrhs, const char* cache_path, void* stream, int* from_cache,
+                             char* choice, int choice_len);
+
 /* --- Batches of independent clouds ------------------------------------------
  * No counterpart in the reference (one cloud per run, src/main.cu:33-200).
  * A batch joins C clouds (each with its own KD tree and block structure) as

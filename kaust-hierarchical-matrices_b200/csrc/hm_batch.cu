@@ -28,7 +28,7 @@ struct hm_batch_s {
   cudaGraphExec_t exec = nullptr;
   const void* g_x = nullptr;
   void* g_y = nullptr;
-  int g_nrhs = 0, g_ldx = 0, g_ldy = 0, g_orig = 0;
+  int g_nrhs = 0, g_ldx = 0, g_ldy = 0, g_orig = 0, g_gen = -1;
   cudaStream_t g_stream = nullptr;
   ~hm_batch_s() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -195,7 +195,8 @@ hm_status hm_batch_matvec(hm_batch b, int nrhs, const float* X, int ldx, float* 
   if (s == nullptr)
     return hm::fail(HM_ERR_INVALID, "hm_batch_matvec: needs a created stream (the legacy stream cannot be captured)");
   const bool same = b->exec && b->g_x == X && b->g_y == Y && b->g_nrhs == nrhs && b->g_ldx == ldx &&
-                    b->g_ldy == ldy && b->g_orig == original_order && b->g_stream == s;
+                    b->g_ldy == ldy && b->g_orig == original_order && b->g_stream == s &&
+                    b->g_gen == b->H->plan_gen;
   if (!same) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
@@ -222,6 +223,7 @@ hm_status hm_batch_matvec(hm_batch b, int nrhs, const float* X, int ldx, float* 
     b->g_ldy = ldy;
     b->g_orig = original_order;
     b->g_stream = s;
+    b->g_gen = b->H->plan_gen;
   }
   HM_CUDA(cudaGraphLaunch(b->exec, s));
   return HM_OK;

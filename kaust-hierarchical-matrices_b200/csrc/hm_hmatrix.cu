@@ -44,7 +44,9 @@ constexpr int kTR = 64;        // rows of a KMM tile
 constexpr int kTC = 64;        // columns per KMM chunk
 constexpr int kKmmThreads = 256;
 constexpr int kOrthThreads = 256;
-constexpr int kMaxCols = 128;  // max basis columns of one block (rank cap + sample block)
+constexpr int kMaxCols = 256;  // max basis columns of one block (rank cap)
+constexpr int kTruncMax = 128; // widest basis the SVD truncation handles (wider: kept as sampled)
+constexpr int kColGroup = 128; // projection columns per sketch launch
 constexpr int kMaxBs = 32;     // max sample block
 
 struct Prob {
@@ -75,6 +77,7 @@ struct KmmArgs {
   int npts, d;
   KernelParams kp;
   int mode;           // 0: Y = A Omega (bs columns); 1: B = A^T Q (k columns)
+  int col0;           // projection: first basis column of this launch (128 per launch)
   int bs;
   uint32_t seed;
   int round;
@@ -91,8 +94,8 @@ struct KmmArgs {
 template <typename W>
 __global__ void __launch_bounds__(kKmmThreads) k_kmm(KmmArgs<W> a) {
   extern __shared__ __align__(16) unsigned char kmm_raw[];
-  W* Wsm = reinterpret_cast<W*>(kmm_raw);          // [kTC][kMaxCols]
-  float* Asm = reinterpret_cast<float*>(Wsm + kTC * kMaxCols);  // [kTC][kTR]
+  W* Wsm = reinterpret_cast<W*>(kmm_raw);          // [kTC][kColGroup]
+  float* Asm = reinterpret_cast<float*>(Wsm + kTC * kColGroup);  // [kTC][kTR]
   float* colc = Asm + kTC * kTR;                   // [d][kTC]
   double* red = reinterpret_cast<double*>(colc + kMaxDim * kTC);  // [kKmmThreads/32]
 
@@ -100,14 +103,15 @@ __global__ void __launch_bounds__(kKmmThreads) k_kmm(KmmArgs<W> a) {
   const Prob P = a.probs[it.x];
   const ProbState S = a.st[it.x];
   if (a.mode == 0 && !S.active) return;
-  const int s = a.mode == 0 ? a.bs : S.k;
+  const int col0 = a.mode ? a.col0 : 0;
+  const int s = min(kColGroup, (a.mode == 0 ? a.bs : S.k) - col0);
   if (s <= 0) return;
   const int mr = a.mode ? P.n : P.m;        // rows of the operator
   const int nc = a.mode ? P.m : P.n;        // columns of the operator
   const int rbase = a.mode ? P.c0 : P.r0;
   const int cbase = a.mode ? P.r0 : P.c0;
-  W* out = a.ws + (a.mode ? P.boff : P.yoff);
-  const W* Q = a.ws + P.qoff;               // mode 1: W = Q (m x k, ld m)
+  W* out = a.ws + (a.mode ? P.boff : P.yoff) + (size_t)col0 * mr;
+  const W* Q = a.ws + P.qoff + (size_t)col0 * P.m;  // mode 1: W = Q (m x k, ld m)
   const int nslab = s <= 32 ? 1 : (s <= 64 ? 2 : 4);
   const int ncg = 4 / nslab;
   const int t = threadIdx.x, r = t & 63, q = t >> 6;
@@ -141,7 +145,7 @@ __global__ void __launch_bounds__(kKmmThreads) k_kmm(KmmArgs<W> a) {
         else
           w = Q[(size_t)cc * P.m + j];
       }
-      Wsm[jj * kMaxCols + cc] = w;
+      Wsm[jj * kColGroup + cc] = w;
     }
     __syncthreads();
     // kernel entries of this thread's row, columns q, q+4, ...
@@ -161,7 +165,7 @@ __global__ void __launch_bounds__(kKmmThreads) k_kmm(KmmArgs<W> a) {
     __syncthreads();
     for (int jj = cg; jj < kTC; jj += ncg) {
       W av = (W)Asm[jj * kTR + r];
-      const W* w = Wsm + jj * kMaxCols + slab * 32;
+      const W* w = Wsm + jj * kColGroup + slab * 32;
 #pragma unroll
       for (int c = 0; c < 32; ++c) acc[c] = fma(av, w[c], acc[c]);
     }
@@ -207,163 +211,6 @@ __global__ void __launch_bounds__(kKmmThreads) k_kmm(KmmArgs<W> a) {
 // W = a Gaussian table whose entries are BF16 numbers, 2 MMAs per tile.
 // Projection pass: W = Q split hi + lo, 3 MMAs per tile (hi*hi, lo*hi, hi*lo).
 // ---------------------------------------------------------------------------
-constexpr int kWS = 136;  // word stride of the staged W pairs (== 8 mod 32: conflict-free fragments)
-
-struct KmmTcArgs {
-  const Prob* probs;
-  ProbState* st;
-  const int2* items;
-  const float* pts;
-  int npts, d;
-  KernelParams kp;
-  int mode;      // 0 sample (bs columns of the Gaussian table), 1 projection (k columns of Q)
-  int bs;
-  int round;
-  const float* omega;  // Gaussian table, [max columns][bs], BF16-exact values
-  int omega_rows;
-  float* ws;
-};
-
-__device__ __forceinline__ float kentry(const KernelParams& kp, const float* rc, const float* cc, int d) {
-  float r2 = 0.f;
-  for (int k = 0; k < d; ++k) {
-    float df = rc[k] - cc[k * kTC];
-    r2 = fmaf(df, df, r2);
-  }
-  return kernel_r2(kp, r2);
-}
-
-__global__ void __launch_bounds__(128) k_kmm_tc(KmmTcArgs a) {
-  __shared__ float colc[kMaxDim * kTC];
-  __shared__ uint32_t Whi[(kTC / 2) * kWS];
-  __shared__ uint32_t Wlo[(kTC / 2) * kWS];
-  __shared__ double red[4];
-  const int2 it = a.items[blockIdx.x];
-  const Prob P = a.probs[it.x];
-  const ProbState S = a.st[it.x];
-  if (a.mode == 0 && !S.active) return;
-  const int s = a.mode == 0 ? a.bs : S.k;
-  if (s <= 0) return;
-  const int mr = a.mode ? P.n : P.m;
-  const int nc = a.mode ? P.m : P.n;
-  const int rbase = a.mode ? P.c0 : P.r0;
-  const int cbase = a.mode ? P.r0 : P.c0;
-  float* out = a.ws + (a.mode ? P.boff : P.yoff);
-  const float* Q = a.ws + P.qoff;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int ra = it.y * kTR + warp * 16 + g, rb = ra + 8;
-  const bool ra_ok = ra < mr, rb_ok = rb < mr;
-  float rca[kMaxDim], rcb[kMaxDim];
-#pragma unroll
-  for (int k = 0; k < kMaxDim; ++k) {
-    rca[k] = (k < a.d && ra_ok) ? a.pts[(size_t)k * a.npts + rbase + ra] : 0.f;
-    rcb[k] = (k < a.d && rb_ok) ? a.pts[(size_t)k * a.npts + rbase + rb] : 0.f;
-  }
-  const int ntiles = (s + 7) >> 3;
-  float acc[16][4];
-#pragma unroll
-  for (int nt = 0; nt < 16; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-  float nrm = 0.f;
-  const bool want_norm = a.mode == 0 && a.round == 0;
-  for (int c0 = 0; c0 < nc; c0 += kTC) {
-    __syncthreads();
-    for (int e = threadIdx.x; e < a.d * kTC; e += blockDim.x) {
-      int k = e / kTC, jj = e % kTC;
-      colc[e] = c0 + jj < nc ? a.pts[(size_t)k * a.npts + cbase + c0 + jj] : 0.f;
-    }
-    // W pairs along the column index: word (jp, n) = {W[2jp][n], W[2jp+1][n]}
-    for (int e = threadIdx.x; e < (kTC / 2) * s; e += blockDim.x) {
-      int n = e / (kTC / 2), jp = e % (kTC / 2);
-      int j0 = c0 + 2 * jp;
-      float w0 = 0.f, w1 = 0.f;
-      if (a.mode == 0) {
-        if (j0 < nc) w0 = a.omega[(size_t)j0 * a.bs + n];
-        if (j0 + 1 < nc) w1 = a.omega[(size_t)(j0 + 1) * a.bs + n];
-        Whi[jp * kWS + n] = pack_bf16(w0, w1);
-      } else {
-        if (j0 < nc) w0 = Q[(size_t)n * P.m + j0];
-        if (j0 + 1 < nc) w1 = Q[(size_t)n * P.m + j0 + 1];
-        uint32_t hi, lo;
-        split_bf16x2(w0, w1, hi, lo);
-        Whi[jp * kWS + n] = hi;
-        Wlo[jp * kWS + n] = lo;
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int ks = 0; ks < kTC / 16; ++ks) {
-      const int cb = ks * 16 + 2 * t;  // columns cb, cb+1, cb+8, cb+9 of the chunk
-      float e[8];
-      const int cols[4] = {cb, cb + 1, cb + 8, cb + 9};
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const bool cok = c0 + cols[q] < nc;
-        e[q] = (ra_ok && cok) ? kentry(a.kp, rca, colc + cols[q], a.d) : 0.f;
-        e[4 + q] = (rb_ok && cok) ? kentry(a.kp, rcb, colc + cols[q], a.d) : 0.f;
-      }
-      if (want_norm) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) nrm = fmaf(e[q], e[q], nrm);
-      }
-      uint32_t ah[4], al[4];
-      split_bf16x2(e[0], e[1], ah[0], al[0]);  // row g, cols cb, cb+1
-      split_bf16x2(e[4], e[5], ah[1], al[1]);  // row g+8
-      split_bf16x2(e[2], e[3], ah[2], al[2]);  // row g, cols cb+8, cb+9
-      split_bf16x2(e[6], e[7], ah[3], al[3]);  // row g+8
-      const int wrow = ks * 8 + t;
-#pragma unroll
-      for (int nt = 0; nt < 16; ++nt) {
-        if (nt < ntiles) {
-          const int n = nt * 8 + g;
-          uint32_t b0 = Whi[wrow * kWS + n], b1 = Whi[(wrow + 4) * kWS + n];
-          float dacc[4] = {0.f, 0.f, 0.f, 0.f};
-          if (a.mode == 1) {
-            uint32_t l0 = Wlo[wrow * kWS + n], l1 = Wlo[(wrow + 4) * kWS + n];
-            mma_bf16(dacc, ah[0], ah[1], ah[2], ah[3], l0, l1);
-          }
-          mma_bf16(dacc, al[0], al[1], al[2], al[3], b0, b1);
-          mma_bf16(dacc, ah[0], ah[1], ah[2], ah[3], b0, b1);
-          add4(acc[nt], dacc);  // round-to-nearest accumulation across k-steps
-        }
-      }
-    }
-  }
-  const int ld = mr;
-#pragma unroll
-  for (int nt = 0; nt < 16; ++nt) {
-    if (nt < ntiles) {
-      const int c = nt * 8 + 2 * t;
-      if (ra_ok) {
-        if (c < s) out[(size_t)c * ld + ra] = acc[nt][0];
-        if (c + 1 < s) out[(size_t)(c + 1) * ld + ra] = acc[nt][1];
-      }
-      if (rb_ok) {
-        if (c < s) out[(size_t)c * ld + rb] = acc[nt][2];
-        if (c + 1 < s) out[(size_t)(c + 1) * ld + rb] = acc[nt][3];
-      }
-    }
-  }
-  if (want_norm) {
-    double dn = nrm;
-    for (int o = 16; o > 0; o >>= 1) dn += __shfl_xor_sync(0xffffffffu, dn, o);
-    if (lane == 0) red[warp] = dn;
-    __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(&a.st[it.x].normA2, red[0] + red[1] + red[2] + red[3]);
-  }
-}
-
-// Gaussian table for one sample round, rounded to BF16 (the rounded values are
-// the test matrix)
-__global__ void k_omega(float* om, int rows, int bs, uint32_t seed, int round) {
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)rows * bs;
-       e += (long long)gridDim.x * blockDim.x) {
-    int j = (int)(e / bs), c = (int)(e % bs);
-    float x = gauss_at(seed, 0x51ed270bu + round, (uint32_t)j, (uint32_t)c);
-    om[e] = __uint_as_float(pack_bf16(x, 0.f) << 16);
-  }
-}
-
-// ---------------------------------------------------------------------------
 // k_kmm_fast: the tensor-core sketch product specialised on the dimension
 // (1-3), the kernel and its derivative.  Coordinates are pre-scaled so that
 // each entry costs one hardware square root and one hardware exp2 (PTX
@@ -389,6 +236,7 @@ struct KmmFastArgs {
   const uint32_t* qh;       // projection: Q pairs [jp][kpad8], hi and lo, per problem
   const uint32_t* ql;
   const long long* qpoff;   // per problem (batch index), words
+  int col0;                 // projection: first basis column of this launch
   float* ws;
 };
 
@@ -434,13 +282,15 @@ __global__ void __launch_bounds__(128) k_kmm_fast(KmmFastArgs a) {
   const Prob P = a.probs[it.x];
   const ProbState S = a.st[it.x];
   if (MODE == 0 && !S.active) return;
-  const int s = MODE == 0 ? a.bs : S.k;
+  const int col0 = MODE ? a.col0 : 0;
+  const int s = (MODE == 0 ? a.bs : S.k) - col0;  // output columns of this launch
   if (s <= 0) return;
   const int mr = MODE ? P.n : P.m;
   const int nc = MODE ? P.m : P.n;
   const int rbase = MODE ? P.c0 : P.r0;
   const int cbase = MODE ? P.r0 : P.c0;
-  float* out = a.ws + (MODE ? P.boff : P.yoff);
+  const int mr_ld = mr;
+  float* out = a.ws + (MODE ? P.boff : P.yoff) + (size_t)col0 * mr_ld;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int ra = it.y * kTR + warp * 16 + g, rb = ra + 8;
   const bool ra_ok = ra < mr, rb_ok = rb < mr;
@@ -452,9 +302,9 @@ __global__ void __launch_bounds__(128) k_kmm_fast(KmmFastArgs a) {
     rcb[k] = rb_ok ? a.pts[(size_t)k * a.npts + rbase + rb] * a.scale : 0.f;
   }
   const int ntiles = min(NT, (s + 7) >> 3);
-  const uint32_t* Bh = MODE ? a.qh + a.qpoff[it.x] : a.om2;
-  const uint32_t* Bl = MODE ? a.ql + a.qpoff[it.x] : nullptr;
-  const size_t ldb = MODE ? (size_t)((s + 7) & ~7) : (size_t)a.ld_om;
+  const uint32_t* Bh = MODE ? a.qh + a.qpoff[it.x] + col0 : a.om2;
+  const uint32_t* Bl = MODE ? a.ql + a.qpoff[it.x] + col0 : nullptr;
+  const size_t ldb = MODE ? (size_t)((S.k + 7) & ~7) : (size_t)a.ld_om;
   float acc[NT][4];
 #pragma unroll
   for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
@@ -614,7 +464,7 @@ void launch_kmm_fast3(int mode, int nt, unsigned grid, cudaStream_t s, const Kmm
     else if (nt <= 8)
       k_kmm_fast<D, KIND, 1, 8><<<grid, 128, 0, s>>>(a);
     else
-      k_kmm_fast<D, KIND, 1, kMaxCols / 8><<<grid, 128, 0, s>>>(a);
+      k_kmm_fast<D, KIND, 1, kColGroup / 8><<<grid, 128, 0, s>>>(a);
   }
 }
 template <int D>
@@ -652,9 +502,10 @@ struct OrthArgs {
 template <typename W>
 __device__ void block_qty(const W* Q, const W* Y, int m, int k, int bs, W* Csm, W* stage) {
   const int t = threadIdx.x;
-  W accv[16];
+  constexpr int kPer = kMaxCols * kMaxBs / kOrthThreads;  // outputs per thread
+  W accv[kPer];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) accv[i] = W(0);
+  for (int i = 0; i < kPer; ++i) accv[i] = W(0);
   W* Qs = stage;                  // [kMaxCols][33]
   W* Ys = stage + kMaxCols * 33;  // [kMaxBs][33]
   const int nout = k * bs;
@@ -669,7 +520,7 @@ __device__ void block_qty(const W* Q, const W* Y, int m, int k, int bs, W* Csm, 
     }
     __syncthreads();
 #pragma unroll
-    for (int x = 0; x < 16; ++x) {
+    for (int x = 0; x < kPer; ++x) {
       int o = t + x * kOrthThreads;
       if (o < nout) {
         int j = o / bs, c = o % bs;
@@ -681,7 +532,7 @@ __device__ void block_qty(const W* Q, const W* Y, int m, int k, int bs, W* Csm, 
     __syncthreads();
   }
 #pragma unroll
-  for (int x = 0; x < 16; ++x) {
+  for (int x = 0; x < kPer; ++x) {
     int o = t + x * kOrthThreads;
     if (o < nout) Csm[o] = accv[x];  // Csm[j*bs + c]
   }
@@ -898,7 +749,7 @@ __global__ void __launch_bounds__(kGramThreads) k_gram_big(const Prob* probs, co
   __shared__ double Bs[16][kMaxCols + 1];
   const int p = blockIdx.x;
   const int k = st[p].k;
-  if (k <= 1) return;
+  if (k <= 1 || k > kTruncMax) return;  // wider bases are kept as sampled
   const Prob P = probs[p];
   const W* B = ws + P.boff;
   const int nt = (k + 7) / 8;
@@ -960,11 +811,12 @@ __global__ void __launch_bounds__(kGramThreads) k_jacobi(const Prob* probs, Prob
   ProbState S = st[p];
   const int k = S.k;
   const int t = threadIdx.x;
-  if (k <= 1) {
+  if (k <= 1 || k > kTruncMax) {
+    // no truncation: W = identity, every column keeps its low part
+    for (int e = t; e < k * k; e += kGramThreads) Wr[goff[p] + e] = (e / k == e % k) ? 1.f : 0.f;
     if (t == 0) {
       st[p].r = k;
       st[p].rhi = k;
-      if (k == 1) Wr[goff[p]] = 1.f;
     }
     return;
   }
@@ -1177,7 +1029,7 @@ __global__ void k_dense_gen(const DenseItem* items, const float* pts, int npts, 
 
 template <typename W>
 size_t kmm_smem() {
-  return sizeof(W) * (kTC * kMaxCols) + sizeof(float) * (kTC * kTR + kMaxDim * kTC) +
+  return sizeof(W) * (kTC * kColGroup) + sizeof(float) * (kTC * kTR + kMaxDim * kTC) +
          sizeof(double) * (kKmmThreads / 32);
 }
 
@@ -1205,7 +1057,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   if (opt.max_rank <= 0) opt.max_rank = 64;
   const int bs = opt.sample_block;
   if (opt.max_rank > kMaxCols || opt.leaf_max_rank > kMaxCols)
-    return fail(HM_ERR_UNSUPPORTED, "hm_hmatrix_build: rank caps must be <= 128");
+    return fail(HM_ERR_UNSUPPORTED, "hm_hmatrix_build: rank caps must be <= 256");
 
   cudaEvent_t ev0, ev1;
   HM_CUDA(cudaEventCreate(&ev0));
@@ -1364,11 +1216,9 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       oa.ws = ws.p;
       oa.bs = bs;
       oa.thresh2 = thresh2;
-      // FP32 working precision: sketch products on the tensor cores
+      // FP32 working precision and d <= 3: specialised tensor-core sketch
+      // kernels; otherwise the SIMT kernel in the working precision
       constexpr bool kTensor = std::is_same<W, float>::value;
-      KmmTcArgs kt;
-      DevBuf<float> omega;
-      // specialised sketch kernels for d <= 3
       const bool fast = kTensor && t->d <= 3;
       KmmFastArgs kf{};
       DevBuf<uint32_t> om2;
@@ -1403,21 +1253,6 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
         kf.ld_om = bs8;
         kf.ws = reinterpret_cast<float*>(ws.p);
       }
-      if constexpr (kTensor) {
-        int max_n = 1;
-        for (const Prob& P : bp) max_n = std::max(max_n, P.n);
-        if ((st = omega.alloc_async((size_t)max_n * bs, stream))) return st;
-        kt.probs = dprobs.p;
-        kt.st = dst.p;
-        kt.pts = t->pts_tree_f.p;
-        kt.npts = t->n;
-        kt.d = t->d;
-        kt.kp = h->kp;
-        kt.bs = bs;
-        kt.omega = omega.p;
-        kt.ws = reinterpret_cast<float*>(ws.p);
-        kt.omega_rows = max_n;
-      }
       tr.mark("batch setup", stream, nb);
       const int max_rounds = kMaxCols / bs + 2;
       for (int round = 0; round < max_rounds; ++round) {
@@ -1430,15 +1265,9 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
           kf.items = drows.p;
           oa.bs = rbs;
           launch_kmm_fast(t->d, opt.kernel, 0, (rbs + 7) / 8, (unsigned)items_rows.size(), stream, kf);
-        } else if constexpr (kTensor) {
-          k_omega<<<592, 256, 0, stream>>>(omega.p, kt.omega_rows, bs, ka.seed, round);
-          HM_LAUNCH_CHECK();
-          kt.mode = 0;
-          kt.round = round;
-          kt.items = drows.p;
-          k_kmm_tc<<<(unsigned)items_rows.size(), 128, 0, stream>>>(kt);
         } else {
           ka.mode = 0;
+          ka.col0 = 0;
           ka.round = round;
           ka.items = drows.p;
           k_kmm<W><<<(unsigned)items_rows.size(), kKmmThreads, kmm_smem<W>(), stream>>>(ka);
@@ -1477,34 +1306,43 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
         kf.qpoff = dqpoff.p;
         // one launch per basis-width class, so the narrow (most) blocks run
         // with few accumulator registers
-        std::vector<int2> cls[3];
+        // (bases wider than 128 columns take a second launch for columns
+        // 128.. of the same items)
+        std::vector<int2> cls[4];
         for (const int2& ic : items_cols) {
           const int kk = hst[ic.x].k;
           if (kk <= 0) continue;
-          cls[kk <= 32 ? 0 : (kk <= 64 ? 1 : 2)].push_back(ic);
+          cls[kk <= 32 ? 0 : (kk <= 64 ? 1 : (kk <= kColGroup ? 2 : 3))].push_back(ic);
         }
-        const int cls_nt[3] = {4, 8, kMaxCols / 8};
+        const int cls_nt[4] = {4, 8, kColGroup / 8, kColGroup / 8};
         size_t ncls = 0;
         for (auto& c : cls) ncls += c.size();
         if ((st = dcls.alloc_async(std::max<size_t>(ncls, 1), stream))) return st;
         size_t o = 0;
-        for (int c = 0; c < 3; ++c) {
+        for (int c = 0; c < 4; ++c) {
           if (cls[c].empty()) continue;
           HM_CUDA(cudaMemcpyAsync(dcls.p + o, cls[c].data(), sizeof(int2) * cls[c].size(), cudaMemcpyHostToDevice,
                                   stream));
           kf.items = dcls.p + o;
-          launch_kmm_fast(t->d, opt.kernel, 1, cls_nt[c], (unsigned)cls[c].size(), stream, kf);
-          HM_LAUNCH_CHECK();
+          for (int c0 = 0; c0 < (c == 3 ? kMaxCols : kColGroup); c0 += kColGroup) {
+            kf.col0 = c0;
+            launch_kmm_fast(t->d, opt.kernel, 1, cls_nt[c], (unsigned)cls[c].size(), stream, kf);
+            HM_LAUNCH_CHECK();
+          }
           o += cls[c].size();
         }
-      } else if constexpr (kTensor) {
-        kt.mode = 1;
-        kt.items = dcols.p;
-        k_kmm_tc<<<(unsigned)items_cols.size(), 128, 0, stream>>>(kt);
+        kf.col0 = 0;
       } else {
         ka.mode = 1;
         ka.items = dcols.p;
-        k_kmm<W><<<(unsigned)items_cols.size(), kKmmThreads, kmm_smem<W>(), stream>>>(ka);
+        int kmx = 0;
+        for (int i = 0; i < nb; ++i) kmx = std::max(kmx, hst[i].k);
+        for (int c0 = 0; c0 < kmx; c0 += kColGroup) {
+          ka.col0 = c0;
+          k_kmm<W><<<(unsigned)items_cols.size(), kKmmThreads, kmm_smem<W>(), stream>>>(ka);
+          HM_LAUNCH_CHECK();
+        }
+        ka.col0 = 0;
       }
       HM_LAUNCH_CHECK();
 
@@ -1518,7 +1356,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       for (int i = 0; i < nb; ++i) {
         goff[i] = (long long)gtot;
         gtot += (size_t)hst[i].k * hst[i].k;
-        kbig = std::max(kbig, hst[i].k);
+        if (hst[i].k <= kTruncMax) kbig = std::max(kbig, hst[i].k);
       }
       DevBuf<long long> dgoff;
       DevBuf<double> Gbuf;
@@ -1530,7 +1368,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       k_gram_big<W><<<nb, kGramThreads, 0, stream>>>(dprobs.p, dst.p, ws.p, dgoff.p, Gbuf.p);
       HM_LAUNCH_CHECK();
       HM_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)jacobi_smem(kMaxCols)));
+                                   (int)jacobi_smem(kTruncMax)));
       // error budget (relative, squared): sampling residual <= 0.09 tol^2 (the
       // stopping test), truncation 0.45 tol^2 (FP32 form) or 0.35 tol^2 plus
       // 0.15 tol^2 of BF16 rounding (mixed form)
@@ -1553,9 +1391,11 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
         long long gi = pstart + i;
         nrm[gi] = S.normA2;
         // a block that missed the tolerance at its rank cap is stored dense when
-        // that is affordable (leaf blocks always are); a large one keeps its
-        // capped factors and is counted as unconverged
-        const bool small = (size_t)P.m * P.n <= 2 * (size_t)(P.m + P.n) * (size_t)std::max(S.k, 1);
+        // that is affordable (leaf blocks always are; others up to 2^22
+        // entries); a larger one keeps its capped factors and is counted as
+        // unconverged
+        const bool small = (size_t)P.m * P.n <=
+                           std::max((size_t)1 << 22, 2 * (size_t)(P.m + P.n) * (size_t)std::max(S.k, 1));
         if (!(S.converged || S.active) && !(P.level == depth || small)) ++unconverged;
         if (S.converged || S.active || !(P.level == depth || small)) {
           du[i] = (long long)chunk_floats;

@@ -79,6 +79,7 @@ struct MatvecPlan {
   int num_leaves = 0;
   int maxleaf = 1;
   DevBuf<float> Xp, Yp;      // permuted copies for original-order calls (n * nrhs_cap)
+  int p1_rows = 256;          // rows of V per phase-1 item (schedule parameter)
   long long bytes_p1 = 0, bytes_p2 = 0;  // FP32 factor bytes read by each phase (+ dense in phase 2)
   long long multi_t_floats = 0;          // projections written by the chunk reduction
 };
@@ -96,6 +97,7 @@ struct hm_hmatrix_s {
   hm::MatvecPlan plan;
   hm::MxPlan mx;                     // mixed precision form (panels of BF16 hi + lo tiles)
   bool diag_fly = false;             // diagonal leaf blocks recomputed from the coordinates per product
+  int plan_gen = 0;                  // bumped whenever the product's plan is rebuilt
   // host mirror of the block list (for export / tests)
   std::vector<hm::LRBlock> h_lr;
   std::vector<hm::DenseBlock> h_dense;

@@ -36,7 +36,6 @@ static __device__ __align__(256) float hm_noalloc_scratch[size_t(4) << 20];
 namespace hm {
 namespace {
 
-constexpr int kP1Rows = 256;
 constexpr int kWarpsPerCta = 4;
 constexpr int kMaxK = 128;
 constexpr int kMaxTiles = kMaxK / 8;
@@ -107,14 +106,15 @@ __device__ __forceinline__ void p1_item(const LRBlock& B, int i_lo, int i_hi, co
 
 __global__ void __launch_bounds__(32 * kWarpsPerCta) k_p1(const P1Item* items, int nitems, const LRBlock* lr,
                                                           const float* __restrict__ X, int ldx, int nr,
-                                                          float* __restrict__ T, float* __restrict__ Tpart) {
+                                                          float* __restrict__ T, float* __restrict__ Tpart,
+                                                          int p1_rows) {
   const int w = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
   if (w >= nitems) return;
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const P1Item it = items[w];
   const LRBlock B = lr[it.block];
-  const int i_lo = it.chunk * kP1Rows;
-  const int i_hi = min(B.n, i_lo + kP1Rows);
+  const int i_lo = it.chunk * p1_rows;
+  const int i_hi = min(B.n, i_lo + p1_rows);
   float* out = it.part >= 0 ? Tpart + it.part : T + B.toff;  // [16][kpad]
   if (B.k <= 8)
     p1_item<1, 8>(B, i_lo, i_hi, X, ldx, nr, out, g, t);
@@ -331,7 +331,7 @@ hm_status run_panel(hm_hmatrix h, int nr, const float* X, int ldx, float* Y, int
   float* Tpart = T + P.t_floats;
   if (P.num_p1 > 0) {
     k_p1<<<(P.num_p1 + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, s>>>(P.p1.p, P.num_p1, P.lr.p, X,
-                                                                                     ldx, nr, T, Tpart);
+                                                                                     ldx, nr, T, Tpart, P.p1_rows);
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_p1", P.bytes_p1 + 4ll * h->n * nr, s);
   }
@@ -353,15 +353,28 @@ hm_status run_panel(hm_hmatrix h, int nr, const float* X, int ldx, float* Y, int
 
 hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   MatvecPlan& P = h->plan;
+  ++h->plan_gen;  // recorded graphs of the old plan are stale
   const int depth = h->depth;
   const int nleaf = 1 << depth;
   const std::vector<int>& lo = h->tree->h_offsets;
   nrhs_cap = 16;
   P.nrhs_cap = nrhs_cap;
   P.num_leaves = nleaf;
+  // device block list: blocks of rank above 128 become pieces of at most
+  // 128 columns (U and V sliced alike), whose products add up
+  std::vector<LRBlock> lr;
+  lr.reserve(h->h_lr.size());
+  for (const LRBlock& b : h->h_lr) {
+    for (int c0 = 0; c0 == 0 || c0 < b.k; c0 += kMaxK) {
+      LRBlock x = b;
+      x.k = std::min(kMaxK, b.k - c0);
+      x.U = b.U + (size_t)c0 * b.m;
+      x.V = b.V + (size_t)c0 * b.n;
+      lr.push_back(x);
+    }
+  }
   long long tk = 0;
-  for (auto& b : h->h_lr) {
-    if (b.k > kMaxK) return fail(HM_ERR_UNSUPPORTED, "matvec: rank above 128");
+  for (auto& b : lr) {
     b.toff = tk;
     tk += 16ll * ((b.k + 7) & ~7);  // T_b^T: 16 right-hand sides x padded rank
   }
@@ -372,10 +385,10 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   std::vector<P1Item> items;
   std::vector<MultiItem> multi;
   long long part = 0;
-  for (size_t i = 0; i < h->h_lr.size(); ++i) {
-    const LRBlock& b = h->h_lr[i];
+  for (size_t i = 0; i < lr.size(); ++i) {
+    const LRBlock& b = lr[i];
     if (b.k <= 0) continue;
-    int nch = (b.n + kP1Rows - 1) / kP1Rows;
+    int nch = (b.n + P.p1_rows - 1) / P.p1_rows;
     const int kpad = (b.k + 7) & ~7;
     for (int c = 0; c < nch; ++c)
       items.push_back(P1Item{(int)i, c, nch == 1 ? -1ll : part + (long long)c * 16 * kpad});
@@ -388,7 +401,7 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   P.num_multi = (int)multi.size();
   P.part_floats = part;
   P.bytes_p1 = P.bytes_p2 = P.multi_t_floats = 0;
-  for (const auto& b : h->h_lr) {
+  for (const auto& b : lr) {
     P.bytes_p1 += 4ll * b.n * b.k;
     P.bytes_p2 += 4ll * b.m * b.k;
   }
@@ -400,12 +413,12 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
     b = (int)(std::lower_bound(lo.begin(), lo.end() - 1, r0 + m) - lo.begin());
   };
   std::vector<int> cnt(nleaf + 1, 0), dcnt(nleaf + 1, 0);
-  std::vector<std::pair<int, int>> ranges(h->h_lr.size()), dranges(h->h_dense.size());
-  for (size_t i = 0; i < h->h_lr.size(); ++i) {
+  std::vector<std::pair<int, int>> ranges(lr.size()), dranges(h->h_dense.size());
+  for (size_t i = 0; i < lr.size(); ++i) {
     int a, e;
-    leaf_range(h->h_lr[i].r0, h->h_lr[i].m, a, e);
+    leaf_range(lr[i].r0, lr[i].m, a, e);
     ranges[i] = {a, e};
-    if (h->h_lr[i].k > 0)
+    if (lr[i].k > 0)
       for (int l = a; l < e; ++l) cnt[l]++;
   }
   for (size_t i = 0; i < h->h_dense.size(); ++i) {
@@ -421,8 +434,8 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   }
   std::vector<int> blk(std::max(ptr[nleaf], 1)), dblk(std::max(dptr[nleaf], 1));
   std::vector<int> fill(ptr.begin(), ptr.end() - 1), dfill(dptr.begin(), dptr.end() - 1);
-  for (size_t i = 0; i < h->h_lr.size(); ++i) {
-    if (h->h_lr[i].k <= 0) continue;
+  for (size_t i = 0; i < lr.size(); ++i) {
+    if (lr[i].k <= 0) continue;
     for (int l = ranges[i].first; l < ranges[i].second; ++l) blk[fill[l]++] = (int)i;
   }
   for (size_t i = 0; i < h->h_dense.size(); ++i)
@@ -432,7 +445,7 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
     for (int r = 0; r < lo[l + 1] - lo[l]; r += 32) groups.push_back(make_int2(l, r));
   P.num_groups = (int)groups.size();
 
-  HM_TRY(P.lr.alloc(std::max<size_t>(h->h_lr.size(), 1)));
+  HM_TRY(P.lr.alloc(std::max<size_t>(lr.size(), 1)));
   HM_TRY(P.p1.alloc(std::max<size_t>(items.size(), 1)));
   HM_TRY(P.multi.alloc(std::max<size_t>(multi.size(), 1)));
   HM_TRY(P.groups.alloc(std::max<size_t>(groups.size(), 1)));
@@ -450,7 +463,7 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
     if (bytes) HM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
     return HM_OK;
   };
-  HM_TRY(up(P.lr.p, h->h_lr.data(), sizeof(LRBlock) * h->h_lr.size()));
+  HM_TRY(up(P.lr.p, lr.data(), sizeof(LRBlock) * lr.size()));
   HM_TRY(up(P.p1.p, items.data(), sizeof(P1Item) * items.size()));
   HM_TRY(up(P.multi.p, multi.data(), sizeof(MultiItem) * multi.size()));
   HM_TRY(up(P.groups.p, groups.data(), sizeof(int2) * groups.size()));

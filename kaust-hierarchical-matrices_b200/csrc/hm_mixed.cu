@@ -22,8 +22,6 @@
 namespace hm {
 namespace {
 
-constexpr int kChunkTiles = 64;  // row tiles (2048 rows) per phase-1 unit
-constexpr int kGroupTiles = 8;   // column tiles per phase-1 unit
 
 __device__ __forceinline__ void mma_a4(float (&d)[4], const uint4& a, uint32_t b0, uint32_t b1) {
   mma_bf16(d, a.x, a.y, a.z, a.w, b0, b1);
@@ -422,7 +420,7 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   const int np = (int)members.size();
   std::vector<MxPanel> panels(np);
   std::vector<int> colL_u(pairs.size()), colH_u(pairs.size()), colL_v(pairs.size()), colH_v(pairs.size());
-  long long tiles = 0, s_tiles = 0, t_tiles = 0;
+  long long tiles = 0, t_tiles = 0;
   for (int p = 0; p < np; ++p) {
     long long sl = 0, sh_ = 0;
     for (const Side& m : members[p]) {
@@ -446,7 +444,6 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
     P.tile0 = leaf_tile0[x0];
     P.nrt = leaf_tile0[x1] - P.tile0;
     P.r0 = lo[x0];
-    P.nchunk = std::max(1, (P.nrt + kChunkTiles - 1) / kChunkTiles);
     P.hi1 = tiles;
     tiles += (long long)P.nrt * P.nct;
     P.lo1 = tiles;
@@ -455,8 +452,6 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
     tiles += (long long)P.nrt * P.nct;
     P.lo2 = tiles;
     tiles += (long long)P.nrt * P.nctl;
-    P.s0 = s_tiles;
-    s_tiles += (long long)P.nchunk * P.nct;
     P.t0 = t_tiles;
     t_tiles += P.nct;
   }
@@ -481,17 +476,6 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
     bytes_lr += 2ll * (q.m + q.n) * (q.k + q.khi);
   }
 
-  // phase-1 units, the largest first
-  std::vector<MxUnit> units;
-  for (int p = 0; p < np; ++p) {
-    const MxPanel& P = panels[p];
-    for (int c = 0; c < P.nct; c += kGroupTiles)
-      for (int ch = 0; ch < P.nchunk; ++ch)
-        units.push_back(MxUnit{p, c, std::min(kGroupTiles, P.nct - c), ch * kChunkTiles,
-                               std::min(kChunkTiles, P.nrt - ch * kChunkTiles), ch});
-  }
-  std::stable_sort(units.begin(), units.end(),
-                   [](const MxUnit& a, const MxUnit& b) { return a.nrt * a.nct > b.nrt * b.nct; });
 
   // ---- dense blocks ----------------------------------------------------------
   std::vector<MxDense> dense;
@@ -530,9 +514,9 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   // ---- upload and convert ----------------------------------------------------
   M.store_tiles = tiles;
   HM_TRY(M.store.alloc((size_t)std::max<long long>(tiles, 1) * 32));
-  HM_TRY(upload(M.panels, panels, s));
+  M.h_panels = panels;
+  HM_TRY(mixed_schedule(h, M.chunk_tiles, M.group_tiles, s));
   HM_TRY(upload(M.pan_of, pan_of, s));
-  HM_TRY(upload(M.units, units, s));
   HM_TRY(upload(M.tile_leaf, tile_leaf, s));
   HM_TRY(upload(M.leaf_tile0, leaf_tile0, s));
   HM_TRY(upload(M.tsrc, tsrc, s));
@@ -540,9 +524,7 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   HM_TRY(upload(M.leaf_dptr, dptr, s));
   HM_TRY(upload(M.leaf_dblk, dblk, s));
   M.num_panels = np;
-  M.num_units = (int)units.size();
   M.num_dense = (int)dense.size();
-  M.s_tiles = s_tiles;
   M.t_tiles = t_tiles;
   // each factor is read once per phase (as V of one orientation in phase 1,
   // as U of the other in phase 2)
@@ -585,6 +567,36 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   }
   HM_CUDA(cudaStreamSynchronize(s));
   M.enabled = true;
+  return HM_OK;
+}
+
+hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, cudaStream_t s) {
+  MxPlan& M = h->mx;
+  if (chunk_tiles < 1 || group_tiles < 1 || group_tiles > 8)
+    return fail(HM_ERR_INVALID, "mixed schedule: need chunk >= 1 and 1 <= group <= 8 column tiles");
+  std::vector<MxPanel>& panels = M.h_panels;
+  long long s_tiles = 0;
+  std::vector<MxUnit> units;
+  for (int p = 0; p < (int)panels.size(); ++p) {
+    MxPanel& P = panels[p];
+    P.nchunk = std::max(1, (P.nrt + chunk_tiles - 1) / chunk_tiles);
+    P.s0 = s_tiles;
+    s_tiles += (long long)P.nchunk * P.nct;
+    for (int c = 0; c < P.nct; c += group_tiles)
+      for (int ch = 0; ch < P.nchunk; ++ch)
+        units.push_back(MxUnit{p, c, std::min(group_tiles, P.nct - c), ch * chunk_tiles,
+                               std::min(chunk_tiles, P.nrt - ch * chunk_tiles), ch});
+  }
+  // the largest units first, so that the small ones fill the tail
+  std::stable_sort(units.begin(), units.end(),
+                   [](const MxUnit& a, const MxUnit& b) { return a.nrt * a.nct > b.nrt * b.nct; });
+  HM_TRY(upload(M.panels, panels, s));
+  HM_TRY(upload(M.units, units, s));
+  HM_CUDA(cudaStreamSynchronize(s));
+  M.num_units = (int)units.size();
+  M.s_tiles = s_tiles;
+  M.chunk_tiles = chunk_tiles;
+  M.group_tiles = group_tiles;
   return HM_OK;
 }
 

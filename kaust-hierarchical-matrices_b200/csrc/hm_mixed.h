@@ -71,6 +71,8 @@ struct MxPlan {
   int num_dense = 0;
   DevBuf<int> leaf_dptr, leaf_dblk;  // dense blocks covering each leaf's rows
   long long bytes_p1 = 0, bytes_p2 = 0;  // BF16 bytes of the factors (unpadded) and dense blocks
+  std::vector<MxPanel> h_panels;          // host copy (the schedule rebuilds units and S offsets)
+  int chunk_tiles = 64, group_tiles = 8;  // phase-1 unit shape (schedule parameters)
   // scratch of one 16-column panel of right-hand sides, in floats
   long long scratch_floats() const { return ((long long)num_tiles * 4 + s_tiles + t_tiles) * 128; }
 };
@@ -92,6 +94,11 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
                       cudaStream_t s);
 
 struct KernelMarks;
+
+// Phase-1 units of chunk_tiles row tiles x group_tiles (<= 8) column tiles,
+// and the projection's S layout that goes with them.  The caller rebuilds the
+// matvec plan afterwards (the scratch size changes).
+hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, cudaStream_t s);
 
 // One panel of nr <= 16 right-hand sides in tree order; scratch holds
 // scratch_floats() floats.  km (optional) receives an event after each kernel.

@@ -106,6 +106,7 @@ def lib():
             L.hm_batch_hmatrix.restype = P
             L.hm_batch_matvec.argtypes = [P, I, P, I, P, I, I, P]
             L.hm_batch_free.argtypes = [P]
+            L.hm_autotune.argtypes = [P, I, ctypes.c_char_p, P, P, ctypes.c_char_p, I]
         _lib = L
     return _lib
 
@@ -353,6 +354,16 @@ class Batch:
             self.free()
         except Exception:
             pass
+
+
+def autotune(H, nrhs=16, cache_path=None, stream=None):
+    """Pick the fastest product schedule for H (hm_autotune); returns
+    (description, taken_from_cache)."""
+    fc = ctypes.c_int()
+    buf = ctypes.create_string_buffer(128)
+    _check(lib().hm_autotune(H.h, nrhs, cache_path.encode() if cache_path else None, _stream(stream),
+                             ctypes.byref(fc), buf, 128))
+    return buf.value.decode(), bool(fc.value)
 
 
 def default_opts(d):

@@ -179,7 +179,7 @@ def test_rejects_bad_options(hm):
     with pytest.raises(hm.HMError):
         hm.build_hmatrix(tree, st, pts, kernel=7)
     with pytest.raises(hm.HMError):
-        hm.build_hmatrix(tree, st, pts, max_rank=200)
+        hm.build_hmatrix(tree, st, pts, max_rank=300)
     with pytest.raises(hm.HMError):
         hm.build_hmatrix(tree, st, pts, sample_block=64)
 
