@@ -52,14 +52,43 @@ def peaks():
     return 6650.0, "fallback"
 
 
+# The workloads: "precision" is the headline (the bench line of a plain
+# `python bench.py`); "scale" and "batch" measure the other two forms.
+WORKLOADS = {
+    "precision": dict(desc="precision form: N=%(n)d uniform 3-D, Matern-3/2 l=0.2 + 1e-3 diag, bucket 64, "
+                           "box-center eta=1, tol 1e-4, rank cap 128, %(nrhs)d RHS",
+                      n=1 << 20, nrhs=16, points="uniform", kernel="matern32", ell=0.2, nugget=1e-3, eta=1.0,
+                      tol=1e-4, max_rank=128),
+    "scale": dict(desc="scale stress: N=%(n)d points of a 16-component Gaussian mixture (sigma log-uniform "
+                       "[0.01, 0.1], Dirichlet(1) weights), exp(-r/0.05), bucket 64, box-center eta=1.5, tol 1e-4, "
+                       "rank cap 256, %(nrhs)d RHS",
+                  n=1 << 21, nrhs=128, points="mixture", kernel="exp", ell=0.05, nugget=0.0, eta=1.5, tol=1e-4,
+                  max_rank=256),
+    "batch": dict(desc="batching form: %(clouds)d clouds of log-uniform [2048, 65536] points (multiples of 32), "
+                       "uniform 3-D, exp(-r/0.1), bucket 64, box-center eta=1, tol 1e-5, rank cap 256, %(nrhs)d RHS "
+                       "per cloud, one graph launch per product",
+                  n=0, nrhs=32, clouds=64, points="uniform", kernel="exp", ell=0.1, nugget=0.0, eta=1.0, tol=1e-5,
+                  max_rank=256),
+}
+KERNEL_IDS = {"exp": 0, "matern32": 1, "gauss": 2}
+
+
+def workload(args):
+    w = dict(WORKLOADS[args.workload])
+    if args.n:
+        w["n"] = args.n
+    if args.nrhs:
+        w["nrhs"] = args.nrhs
+    return w
+
+
 def workload_config(args):
-    return {
-        "workload": "precision form: N=%d uniform 3-D, Matern-3/2 l=0.2 + 1e-3 diag, bucket 64, "
-                    "box-center eta=1, tol 1e-4, rank cap 128, %d RHS" % (args.n, args.nrhs),
-        "n": args.n, "d": 3, "bucket": 64, "eta": 1.0, "kernel": "matern32", "ell": 0.2, "nugget": 1e-3,
-        "tol": 1e-4, "max_rank": 128, "sample_block": 16, "nrhs": args.nrhs,
-        "l2": "no flush: the streamed H-matrix (GBs) exceeds the 126 MB L2",
-    }
+    w = workload(args)
+    cfg = {"workload": w["desc"] % w, "name": args.workload}
+    cfg.update({k: v for k, v in w.items() if k != "desc"})
+    cfg.update({"d": 3, "bucket": 64, "sample_block": 16,
+                "l2": "no flush: the streamed H-matrix (GBs) exceeds the 126 MB L2"})
+    return cfg
 
 
 class ClockSampler:
@@ -117,8 +146,9 @@ def cpu_reference(args, n, nrhs, budget_s, threads):
     t0 = time.time()
     while time.time() - t0 < budget_s and done_rows < n:
         r0 = int(rng.integers(0, n - rows_per_panel))
-        _, tg, tb = oracle.cpu_panel_matvec(pts, n, 3, perm, oracle.K_MATERN32, 0.2, 1e-3, r0, rows_per_panel, X,
-                                            threads, work)
+        w = workload(args)
+        _, tg, tb = oracle.cpu_panel_matvec(pts, n, 3, perm, KERNEL_IDS[w["kernel"]], w["ell"], w["nugget"], r0,
+                                            rows_per_panel, X, threads, work)
         t_gen += tg
         t_blas += tb
         done_rows += rows_per_panel
@@ -132,15 +162,26 @@ def run_reference(args):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    n, nrhs = args.n, args.nrhs
-    dense_bytes = 8.0 * n * n + 8.0 * n * nrhs * 2
+    w = workload(args)
+    nrhs = w["nrhs"]
+    if args.workload == "batch":
+        # every cloud's dense product; the cost per entry is sampled on the
+        # largest cloud and scaled by sum n_c^2
+        sizes = batch_sizes(w, 2024)
+        n = max(sizes)
+        scale = float(sum(x * x for x in sizes)) / (n * n)
+        dense_bytes = float(sum(8.0 * x * x + 16.0 * x * nrhs for x in sizes))
+    else:
+        n = w["n"]
+        scale = 1.0
+        dense_bytes = 8.0 * n * n + 8.0 * n * nrhs * 2
     vals = []
     # each step is a bounded sample of the product, sized so that the whole
     # run stays within about two minutes whatever --steps is
     per_step = max(0.2, min(args.ref_budget, 120.0 / (args.warmup + args.steps)))
     for _ in range(args.warmup + args.steps):
         t_full, sample, tg, tb, rows = cpu_reference(args, n, nrhs, per_step, threads)
-        vals.append(t_full)
+        vals.append(t_full * scale)
     t = float(np.mean(vals[args.warmup:]))
     value = dense_bytes / t / 1e9
     line = {
@@ -214,7 +255,9 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
-    n, d, b, nrhs = args.n, 3, 64, args.nrhs
+    w = workload(args)
+    n, d, b, nrhs = w["n"], 3, 64, w["nrhs"]
+    kid = KERNEL_IDS[w["kernel"]]
     lib = hm.lib()
 
     def barrier():
@@ -232,9 +275,12 @@ def run_ours(args):
 
     # ---- build: points, KD tree, structure, then each form's H-matrix ---------
     def front():
-        pts = hm.generate_dataset(n, d, seed=1234 + rank, stream=stream)
+        if w["points"] == "mixture":
+            pts = hm.generate_mixture(n, d, ncomp=16, sigma_min=0.01, sigma_max=0.1, seed=1234 + rank, stream=stream)
+        else:
+            pts = hm.generate_dataset(n, d, seed=1234 + rank, stream=stream)
         tree = hm.construct_kdtree(pts, n, d, b, stream=stream)
-        st = hm.construct_hmatrix_structure(tree, hm.BOX_CENTER, 1.0, stream=stream)
+        st = hm.construct_hmatrix_structure(tree, hm.BOX_CENTER, w["eta"], stream=stream)
         return pts, tree, st
 
     (pts, tree, st), front_s = ev_time(front)
@@ -242,9 +288,9 @@ def run_ours(args):
     Hs, build_s = {}, {}
     for f in forms:
         prec = hm.PREC_MIXED if f == "mixed" else hm.PREC_FP32
-        Hs[f], t = ev_time(lambda: hm.build_hmatrix(tree, st, pts, kernel=hm.K_MATERN32, ell=0.2, nugget=1e-3,
-                                                    tol=1e-4, max_rank=128, sample_block=16, precision=prec,
-                                                    seed=7, stream=stream))
+        Hs[f], t = ev_time(lambda: hm.build_hmatrix(tree, st, pts, kernel=kid, ell=w["ell"], nugget=w["nugget"],
+                                                    tol=w["tol"], max_rank=w["max_rank"], sample_block=16,
+                                                    precision=prec, seed=7, stream=stream))
         build_s[f] = front_s + t
     head = forms[0]
 
@@ -286,14 +332,20 @@ def run_ours(args):
     clocks = ClockSampler(os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % rank)
                           if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp/bench_clocks_%d.csv" % rank)
     res = {}
+    nr = min(16, nrhs)  # the product runs in panels of 16 right-hand sides
+    panels = (nrhs + 15) // 16
     for f in forms:
         ms = timed(step_of(Hs[f]), clocks if f == head else None)
-        kt = kernel_times(hm, lib, Hs[f], X, Y, n, nrhs, stream)
+        kt = kernel_times(hm, lib, Hs[f], X, Y, n, nr, stream)
         bp, be = ctypes.c_longlong(), ctypes.c_longlong()
         mp, me = ctypes.c_float(), ctypes.c_float()
-        hm._check(lib.hm_hmatvec_profile(Hs[f].h, nrhs, hm._ptr(X), n, hm._ptr(Y), n, hm._stream(stream),
+        hm._check(lib.hm_hmatvec_profile(Hs[f].h, nr, hm._ptr(X), n, hm._ptr(Y), n, hm._stream(stream),
                                          ctypes.byref(mp), ctypes.byref(me), ctypes.byref(bp), ctypes.byref(be)))
-        res[f] = {"ms": ms, "bytes": bp.value + be.value, "kernels": kt, "launches_per_step": len(kt)}
+        # algorithmic bytes of the whole product: factors and dense blocks once
+        # per phase, X and Y for every right-hand side (12 bytes per row each)
+        by = bp.value + be.value + 12 * n * (nrhs - nr)
+        res[f] = {"ms": ms, "bytes": by, "kernels": kt, "launches_per_step": len(kt) * panels,
+                  "panels": panels}
 
     # ---- roofline of the headline form's dominant kernel --------------------
     hbm, peak_kind = peaks()
@@ -329,7 +381,7 @@ def run_ours(args):
         p_h = pts.cpu().numpy()
         rows = np.random.default_rng(5).choice(n, args.check_rows, replace=False)
         Xn = X.cpu().numpy().astype(np.float64)
-        Yref = oracle.dense_rows_matvec(p_h, n, d, perm, oracle.K_MATERN32, 0.2, 1e-3, rows, Xn)
+        Yref = oracle.dense_rows_matvec(p_h, n, d, perm, kid, w["ell"], w["nugget"], rows, Xn)
         for f in forms:
             step_of(Hs[f])()
             torch.cuda.synchronize()
@@ -360,7 +412,7 @@ def run_ours(args):
             "roofline": roof, "cpu_baseline": cpu,
             "e2e": {"value": world * r["bytes"] / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": 4 * n * nrhs, "d2h_bytes_per_step": 4 * n * nrhs},
-            "gpu_launches": r["launches_per_step"] * args.steps * ((nrhs + 15) // 16),
+            "gpu_launches": r["launches_per_step"] * args.steps,
             "clocks": clocks.summary(local),
         }
         if "fp32" in res and head != "fp32":
@@ -378,14 +430,194 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def batch_sizes(w, seed):
+    """Cloud sizes log-uniform in [2048, 65536], rounded to multiples of 32."""
+    rng = np.random.default_rng(seed)
+    x = np.exp(rng.uniform(np.log(2048), np.log(65536), w["clouds"]))
+    return [int(max(32, round(v / 32) * 32)) for v in x]
+
+
+def run_batch(args):
+    """Batching form: all clouds in one forest, one graph launch per product."""
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+
+    import hmatrix as hm
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    s = torch.cuda.Stream(dev)  # a created stream: the product is a recorded graph
+    w = workload(args)
+    nrhs, kid = w["nrhs"], KERNEL_IDS[w["kernel"]]
+    sizes = batch_sizes(w, 2024 + rank)
+    lib = hm.lib()
+
+    def ev_time(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return out, time.perf_counter() - t0
+
+    def front():
+        cl = []
+        for i, n in enumerate(sizes):
+            pts = hm.generate_dataset(n, 3, seed=5000 + 100 * rank + i, stream=s)
+            tree = hm.construct_kdtree(pts, n, 3, 64, stream=s)
+            st = hm.construct_hmatrix_structure(tree, hm.BOX_CENTER, w["eta"], stream=s)
+            cl.append((n, pts, tree, st))
+        return cl
+
+    with torch.cuda.stream(s):
+        clouds, front_s = ev_time(front)
+        forms = ["mixed", "fp32"] if args.precision == "both" else [args.precision]
+        Bs, build_s, tune = {}, {}, {}
+        cache = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp",
+                             "hm_autotune.txt")
+        for f in forms:
+            B = hm.Batch([c[2] for c in clouds], [c[3] for c in clouds], stream=s)
+            prec = hm.PREC_MIXED if f == "mixed" else hm.PREC_FP32
+            _, t = ev_time(lambda: B.build(kernel=kid, ell=w["ell"], nugget=w["nugget"], tol=w["tol"],
+                                           max_rank=w["max_rank"], precision=prec, seed=7, stream=s))
+            build_s[f] = front_s + t
+            tune[f] = hm.autotune(B.hmatrix(), 16, cache, stream=s)
+            Bs[f] = B
+        head = forms[0]
+        N = Bs[head].n
+        X = torch.randn((nrhs, N), device=dev).t()
+        Y = torch.empty((nrhs, N), device=dev).t()
+        clocks = ClockSampler(os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % rank)
+                              if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp/bench_clocks_%d.csv" % rank)
+        res = {}
+        for f in forms:
+            B = Bs[f]
+            if f == head:
+                clocks.__enter__()
+                time.sleep(0.5)
+            for _ in range(args.warmup):
+                B.matvec(X, Y, s)
+            s.synchronize()
+            if world > 1:
+                dist.barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            for _ in range(args.steps):
+                B.matvec(X, Y, s)
+            e1.record(s)
+            s.synchronize()
+            if f == head:
+                clocks.__exit__()
+            ms = e0.elapsed_time(e1) / args.steps
+            if world > 1:
+                tt = torch.tensor([ms], device=dev)
+                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+                ms = float(tt.item())
+            H = B.hmatrix()
+            kt = kernel_times(hm, lib, H, X, Y, N, 16, s)
+            bp, be = ctypes.c_longlong(), ctypes.c_longlong()
+            mp, me = ctypes.c_float(), ctypes.c_float()
+            hm._check(lib.hm_hmatvec_profile(H.h, 16, hm._ptr(X), N, hm._ptr(Y), N, hm._stream(s), ctypes.byref(mp),
+                                             ctypes.byref(me), ctypes.byref(bp), ctypes.byref(be)))
+            res[f] = {"ms": ms, "bytes": bp.value + be.value + 12 * N * (nrhs - 16), "kernels": kt,
+                      "panels": (nrhs + 15) // 16, "stats": H.stats()}
+        # e2e: host X in, host Y out, product through hm_batch_matvec
+        B = Bs[head]
+        Xh = torch.empty((nrhs, N), pin_memory=True)
+        Xh.copy_(X.t().cpu())
+        Yh = torch.empty((nrhs, N), pin_memory=True)
+        Xd = torch.empty((nrhs, N), device=dev)
+        for _ in range(args.warmup + 1):
+            Xd.copy_(Xh, non_blocking=True)
+            B.matvec(Xd.t(), Y, s)
+            Yh.copy_(Y.t(), non_blocking=True)
+        s.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(args.steps):
+            Xd.copy_(Xh, non_blocking=True)
+            B.matvec(Xd.t(), Y, s)
+            Yh.copy_(Y.t(), non_blocking=True)
+        e1.record(s)
+        s.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / args.steps
+        # accuracy on sampled rows of a few clouds against the FP64 oracle
+        errs = {}
+        if rank == 0 and not args.skip_check:
+            import oracle
+
+            rng = np.random.default_rng(9)
+            pick = rng.choice(len(clouds), 4, replace=False)
+            for f in forms:
+                Bs[f].matvec(X, Y, s)
+                s.synchronize()
+                Yn = Y.cpu().numpy()
+                num = den = 0.0
+                for c in pick:
+                    n, pts, tree, st = clouds[c]
+                    r0, r1 = Bs[f].row_offsets[c], Bs[f].row_offsets[c + 1]
+                    perm = tree.copy_out()["perm"]
+                    rows = rng.choice(n, 64, replace=False)
+                    Xc = X[r0:r1].cpu().numpy().astype(np.float64)
+                    Yref = oracle.dense_rows_matvec(pts.cpu().numpy(), n, 3, perm, kid, w["ell"], w["nugget"], rows,
+                                                    Xc.T).T
+                    num += float(np.sum((Yn[r0:r1][rows] - Yref) ** 2))
+                    den += float(np.sum(Yref ** 2))
+                errs[f] = (num / den) ** 0.5
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        r = res[head]
+        value = world * r["bytes"] / (r["ms"] * 1e-3) / 1e9
+        dom = max(r["kernels"], key=lambda x: x[1])
+        ach = dom[2] / (dom[1] * 1e-3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 hi+lo, f32 acc" if head == "mixed" else "f32", "data": "synthetic",
+            "config": dict(workload_config(args), n_total=N, cloud_sizes=sizes, precision=head,
+                           bytes_per_step=r["bytes"], schedule=tune[head][0]),
+            "hbm_frac": value / world / hbm, "build_s": build_s[head], "rel_err_vs_fp64": errs.get(head),
+            "hbuild": r["stats"],
+            "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": ach, "peak": hbm, "unit": "GB/s",
+                         "frac": ach / hbm, "peak_kind": peak_kind, "traffic": None,
+                         "kernels": {k: {"ms": t, "bytes": by} for k, t, by in r["kernels"]}},
+            "cpu_baseline": None,
+            "e2e": {"value": world * r["bytes"] / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": 4 * N * nrhs, "d2h_bytes_per_step": 4 * N * nrhs},
+            "gpu_launches": len(r["kernels"]) * r["panels"] * args.steps,
+            "graph_launches_per_step": 1,
+            "clocks": clocks.summary(local),
+        }
+        if "fp32" in res and head != "fp32":
+            f = res["fp32"]
+            line["fp32_form"] = {"ms_per_step": f["ms"], "gbs": f["bytes"] / (f["ms"] * 1e-3) / 1e9,
+                                 "build_s": build_s["fp32"], "rel_err_vs_fp64": errs.get("fp32"),
+                                 "schedule": tune["fp32"][0]}
+            line["speedup_vs_fp32"] = f["ms"] / r["ms"]
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=1 << 20)
-    ap.add_argument("--nrhs", type=int, default=16)
+    ap.add_argument("--workload", default="precision", choices=sorted(WORKLOADS),
+                    help="precision (default, the headline line), scale, or batch")
+    ap.add_argument("--n", type=int, default=None, help="points (default: the workload's)")
+    ap.add_argument("--nrhs", type=int, default=None, help="right-hand sides (default: the workload's)")
     ap.add_argument("--precision", default="both", choices=["both", "fp32", "mixed"],
                     help="both: the mixed form is the headline, the FP32 form is timed beside it")
     ap.add_argument("--check-rows", type=int, default=256)
@@ -397,6 +629,8 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
     else:
         run_ours(args)
 

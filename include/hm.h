@@ -84,6 +84,14 @@ HM_API const char* hm_version(void);
 HM_API hm_status hm_generate_dataset(int n, int d, unsigned long long seed, double* d_points,
                               void* stream);
 
+/* Points from an isotropic Gaussian mixture (no counterpart in the reference;
+ * the scale-stress workload): ncomp components with centres uniform in
+ * [0,1]^d, standard deviations log-uniform in [sigma_min, sigma_max] and
+ * weights from Dirichlet(1, ..., 1), all drawn from `seed`; d_points gets the
+ * SoA layout of hm_generate_dataset (d * n doubles). */
+HM_API hm_status hm_generate_mixture(int n, int d, int ncomp, double sigma_min, double sigma_max,
+                                     unsigned long long seed, double* d_points, void* stream);
+
 /* --- KD tree ------------------------------------------------------------ */
 
 /* allocateKDTree + constructKDTree, FULL_TREE division

@@ -2,10 +2,14 @@
 // point generation.
 #include <curand_kernel.h>
 
+#include <cmath>
+#include <vector>
+
 #include <cstdio>
 #include <string>
 
 #include "hm_internal.h"
+#include "hm_kernels.cuh"
 
 namespace hm {
 
@@ -37,6 +41,20 @@ __global__ void k_generate_dataset(long long count, unsigned long long seed, dou
   out[i] = curand_uniform(&s);
 }
 
+// Gaussian mixture point i, coordinate k: component by inverse CDF of the
+// weights at a uniform draw, then centre + sigma * N(0,1); both draws from the
+// counter-based hash generator (seed, point, coordinate).
+__global__ void k_generate_mixture(int n, int d, int ncomp, uint32_t seed, const double* cum, const double* ctr,
+                                   const double* sig, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double u = (mix32(seed ^ mix32((uint32_t)i * 0x9e3779b9u + 0x632be5abu)) >> 8) * (1.0 / 16777216.0);
+  int c = 0;
+  while (c + 1 < ncomp && u >= cum[c]) ++c;
+  for (int k = 0; k < d; ++k)
+    out[(size_t)k * n + i] = ctr[c * d + k] + sig[c] * (double)gauss_at(seed, 0x7f4a7c15u, (uint32_t)i, (uint32_t)k);
+}
+
 hm_status kdtree_build(const double* d_points, int n, int d, int bucket, cudaStream_t stream,
                        hm_kdtree* out);
 hm_status structure_build(hm_kdtree t, int admiss, double eta, cudaStream_t stream,
@@ -60,6 +78,50 @@ hm_status hm_generate_dataset(int n, int d, unsigned long long seed, double* d_p
   hm::k_generate_dataset<<<(unsigned)blocks, threads, 0, hm::as_stream(stream)>>>(count, seed,
                                                                                 d_points);
   HM_LAUNCH_CHECK();
+  return HM_OK;
+}
+
+hm_status hm_generate_mixture(int n, int d, int ncomp, double sigma_min, double sigma_max,
+                              unsigned long long seed, double* d_points, void* stream) {
+  if (!d_points) return hm::fail(HM_ERR_INVALID, "hm_generate_mixture: d_points is NULL");
+  if (n < 1 || d < 1 || ncomp < 1 || !(sigma_min > 0) || !(sigma_max >= sigma_min))
+    return hm::fail(HM_ERR_INVALID, "hm_generate_mixture: need n, d, ncomp >= 1 and 0 < sigma_min <= sigma_max");
+  // component parameters on the host from a splitmix64 stream of the seed
+  uint64_t state = seed ^ 0x2545f4914f6cdd1dull;
+  auto next = [&]() {
+    uint64_t z = (state += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);  // [0, 1)
+  };
+  std::vector<double> ctr((size_t)ncomp * d), sig(ncomp), w(ncomp), cum(ncomp);
+  for (auto& x : ctr) x = next();
+  const double a = std::log(sigma_min), b = std::log(sigma_max);
+  for (auto& x : sig) x = std::exp(a + (b - a) * next());
+  double tot = 0;  // Dirichlet(1, ..., 1): normalised Exp(1) draws
+  for (auto& x : w) {
+    x = -std::log(1.0 - next());
+    tot += x;
+  }
+  double run = 0;
+  for (int c = 0; c < ncomp; ++c) {
+    run += w[c] / tot;
+    cum[c] = run;
+  }
+  cum[ncomp - 1] = 1.0;
+  cudaStream_t s = hm::as_stream(stream);
+  hm::DevBuf<double> dcum, dctr, dsig;
+  HM_TRY(dcum.alloc_async(ncomp, s));
+  HM_TRY(dctr.alloc_async(ctr.size(), s));
+  HM_TRY(dsig.alloc_async(ncomp, s));
+  HM_CUDA(cudaMemcpyAsync(dcum.p, cum.data(), 8 * cum.size(), cudaMemcpyHostToDevice, s));
+  HM_CUDA(cudaMemcpyAsync(dctr.p, ctr.data(), 8 * ctr.size(), cudaMemcpyHostToDevice, s));
+  HM_CUDA(cudaMemcpyAsync(dsig.p, sig.data(), 8 * sig.size(), cudaMemcpyHostToDevice, s));
+  hm::k_generate_mixture<<<(n + 255) / 256, 256, 0, s>>>(n, d, ncomp, (uint32_t)(seed ^ (seed >> 32)), dcum.p,
+                                                        dctr.p, dsig.p, d_points);
+  HM_LAUNCH_CHECK();
+  HM_CUDA(cudaStreamSynchronize(s));
   return HM_OK;
 }
 

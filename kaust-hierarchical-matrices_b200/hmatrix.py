@@ -79,6 +79,7 @@ def lib():
         L.hm_last_error.restype = ctypes.c_char_p
         L.hm_version.restype = ctypes.c_char_p
         L.hm_generate_dataset.argtypes = [I, I, ctypes.c_ulonglong, P, P]
+        L.hm_generate_mixture.argtypes = [I, I, I, D, D, ctypes.c_ulonglong, P, P]
         L.hm_kdtree_build.argtypes = [P, I, I, I, P, ctypes.POINTER(P)]
         L.hm_kdtree_info.argtypes = [P, P, P, P, P]
         L.hm_kdtree_copy_out.argtypes = [P, P, P, P, P, P]
@@ -172,6 +173,16 @@ class KDTree:
             self.free()
         except Exception:
             pass
+
+
+def generate_mixture(n, d, ncomp=16, sigma_min=0.01, sigma_max=0.1, seed=1, out=None, stream=None):
+    """Points of an isotropic Gaussian mixture (hm_generate_mixture), SoA float64."""
+    import torch
+
+    if out is None:
+        out = torch.empty(n * d, dtype=torch.float64, device="cuda")
+    _check(lib().hm_generate_mixture(n, d, ncomp, sigma_min, sigma_max, seed, _ptr(out), _stream(stream)))
+    return out
 
 
 def construct_kdtree(points, n, d, bucket, stream=None):
