@@ -244,6 +244,7 @@ def run_ours(args):
     import torch.distributed as dist
 
     import hmatrix as hm
+    import ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -276,9 +277,10 @@ def run_ours(args):
     # ---- build: points, KD tree, structure, then each form's H-matrix ---------
     def front():
         if w["points"] == "mixture":
-            pts = hm.generate_mixture(n, d, ncomp=16, sigma_min=0.01, sigma_max=0.1, seed=1234 + rank, stream=stream)
+            pts = hm.generate_mixture(n, d, ncomp=16, sigma_min=0.01, sigma_max=0.1, seed=ranks.cloud_seed(1234, rank),
+                                      stream=stream)
         else:
-            pts = hm.generate_dataset(n, d, seed=1234 + rank, stream=stream)
+            pts = hm.generate_dataset(n, d, seed=ranks.cloud_seed(1234, rank), stream=stream)
         tree = hm.construct_kdtree(pts, n, d, b, stream=stream)
         st = hm.construct_hmatrix_structure(tree, hm.BOX_CENTER, w["eta"], stream=stream)
         return pts, tree, st
@@ -322,12 +324,7 @@ def run_ours(args):
         if sampler is not None:
             sampler.__exit__()
         barrier()
-        ms = t0.elapsed_time(t1) / args.steps
-        if world > 1:
-            tt = torch.tensor([ms], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms = float(tt.item())
-        return ms
+        return ranks.max_over_ranks(t0.elapsed_time(t1) / args.steps, world)
 
     clocks = ClockSampler(os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % rank)
                           if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp/bench_clocks_%d.csv" % rank)
@@ -398,7 +395,7 @@ def run_ours(args):
 
     if rank == 0:
         r = res[head]
-        value = world * r["bytes"] / (r["ms"] * 1e-3) / 1e9
+        value = ranks.weak_value(r["bytes"], r["ms"], world)
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["ms"], "higher_is_better": True, "scaling": "weak",
@@ -445,6 +442,7 @@ def run_batch(args):
     import torch.distributed as dist
 
     import hmatrix as hm
+    import ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -516,11 +514,7 @@ def run_batch(args):
             s.synchronize()
             if f == head:
                 clocks.__exit__()
-            ms = e0.elapsed_time(e1) / args.steps
-            if world > 1:
-                tt = torch.tensor([ms], device=dev)
-                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-                ms = float(tt.item())
+            ms = ranks.max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
             H = B.hmatrix()
             kt = kernel_times(hm, lib, H, X, Y, N, 16, s)
             bp, be = ctypes.c_longlong(), ctypes.c_longlong()
@@ -548,7 +542,7 @@ def run_batch(args):
             Yh.copy_(Y.t(), non_blocking=True)
         e1.record(s)
         s.synchronize()
-        e2e_ms = e0.elapsed_time(e1) / args.steps
+        e2e_ms = ranks.max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
         # accuracy on sampled rows of a few clouds against the FP64 oracle
         errs = {}
         if rank == 0 and not args.skip_check:
@@ -575,7 +569,7 @@ def run_batch(args):
     if rank == 0:
         hbm, peak_kind = peaks()
         r = res[head]
-        value = world * r["bytes"] / (r["ms"] * 1e-3) / 1e9
+        value = ranks.weak_value(r["bytes"], r["ms"], world)
         dom = max(r["kernels"], key=lambda x: x[1])
         ach = dom[2] / (dom[1] * 1e-3) / 1e9
         line = {
