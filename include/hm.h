@@ -263,6 +263,10 @@ HM_API void hm_hmatrix_free(hm_hmatrix h);
 HM_API hm_status hm_autotune(hm_hmatrix h, int nrhs, const char* cache_path, void* stream, int* from_cache,
                              char* choice, int choice_len);
 
+/* Applies a schedule given as hm_autotune describes it, e.g.
+ * "mixed chunk_tiles=64 group_tiles=8 p1_ring=1" or "fp32 p1_rows=256". */
+HM_API hm_status hm_schedule_set(hm_hmatrix h, const char* choice, void* stream);
+
 /* --- Batches of independent clouds ------------------------------------------
  * No counterpart in the reference (one cloud per run, src/main.cu:33-200).
  * A batch joins C clouds (each with its own KD tree and block structure) as

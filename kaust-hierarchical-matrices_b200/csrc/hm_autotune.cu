@@ -24,13 +24,13 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream);
 namespace {
 
 struct Choice {
-  int a = 0, b = 0;  // FP32: (p1 rows, 0); mixed: (chunk tiles, group tiles)
+  int a = 0, b = 0, c = 0;  // FP32: (p1 rows, 0, 0); mixed: (chunk tiles, group tiles, ring phase 1)
 };
 
 std::string describe(hm_hmatrix h, const Choice& c) {
   char buf[96];
   if (h->mx.enabled)
-    std::snprintf(buf, sizeof buf, "mixed chunk_tiles=%d group_tiles=%d", c.a, c.b);
+    std::snprintf(buf, sizeof buf, "mixed chunk_tiles=%d group_tiles=%d p1_ring=%d", c.a, c.b, c.c);
   else
     std::snprintf(buf, sizeof buf, "fp32 p1_rows=%d", c.a);
   return buf;
@@ -38,7 +38,7 @@ std::string describe(hm_hmatrix h, const Choice& c) {
 
 hm_status apply(hm_hmatrix h, const Choice& c, cudaStream_t s) {
   if (h->mx.enabled) {
-    HM_TRY(mixed_schedule(h, c.a, c.b, s));
+    HM_TRY(mixed_schedule(h, c.a, c.b, c.c, s));
   } else {
     h->plan.p1_rows = c.a;
   }
@@ -68,7 +68,7 @@ bool lookup(const char* path, const std::string& key, Choice* c) {
     std::istringstream ls(line);
     std::string k;
     Choice x;
-    if ((ls >> k >> x.a >> x.b) && k == key) {
+    if ((ls >> k >> x.a >> x.b >> x.c) && k == key) {
       *c = x;
       found = true;
     }
@@ -91,10 +91,11 @@ extern "C" hm_status hm_autotune(hm_hmatrix h, int nrhs, const char* cache_path,
   if (!cached) {
     std::vector<Choice> cand;
     if (h->mx.enabled) {
-      for (int ch : {16, 32, 64, 128})
-        for (int g : {4, 8}) cand.push_back(Choice{ch, g});
+      for (int ring : {1, 0})
+        for (int ch : {16, 32, 64, 128})
+          for (int g : {4, 8}) cand.push_back(Choice{ch, g, ring});
     } else {
-      for (int r : {128, 256, 512, 1024}) cand.push_back(Choice{r, 0});
+      for (int r : {128, 256, 512, 1024}) cand.push_back(Choice{r, 0, 0});
     }
     DevBuf<float> X, Y;
     HM_TRY(X.alloc((size_t)h->n * nrhs));
@@ -130,7 +131,7 @@ extern "C" hm_status hm_autotune(hm_hmatrix h, int nrhs, const char* cache_path,
     if (cache_path) {
       std::ofstream f(cache_path, std::ios::app);
       if (!f) return fail(HM_ERR_INVALID, std::string("hm_autotune: cannot write the cache ") + cache_path);
-      f << key << " " << best.a << " " << best.b << " " << best_ms << "\n";
+      f << key << " " << best.a << " " << best.b << " " << best.c << " " << best_ms << "\n";
     }
   }
   HM_TRY(apply(h, best, s));
@@ -141,4 +142,18 @@ extern "C" hm_status hm_autotune(hm_hmatrix h, int nrhs, const char* cache_path,
     choice[choice_len - 1] = '\0';
   }
   return HM_OK;
+}
+
+extern "C" hm_status hm_schedule_set(hm_hmatrix h, const char* choice, void* stream) {
+  using namespace hm;
+  if (!h || !choice) return fail(HM_ERR_INVALID, "hm_schedule_set: null argument");
+  Choice c;
+  if (h->mx.enabled) {
+    if (std::sscanf(choice, "mixed chunk_tiles=%d group_tiles=%d p1_ring=%d", &c.a, &c.b, &c.c) != 3)
+      return fail(HM_ERR_INVALID, std::string("hm_schedule_set: not a mixed-form schedule: ") + choice);
+  } else {
+    if (std::sscanf(choice, "fp32 p1_rows=%d", &c.a) != 1 || c.a < 16)
+      return fail(HM_ERR_INVALID, std::string("hm_schedule_set: not an FP32-form schedule: ") + choice);
+  }
+  return apply(h, c, as_stream(stream));
 }

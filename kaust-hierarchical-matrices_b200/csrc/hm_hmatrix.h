@@ -79,7 +79,7 @@ struct MatvecPlan {
   int num_leaves = 0;
   int maxleaf = 1;
   DevBuf<float> Xp, Yp;      // permuted copies for original-order calls (n * nrhs_cap)
-  int p1_rows = 256;          // rows of V per phase-1 item (schedule parameter)
+  int p1_rows = 1024;         // rows of V per phase-1 item (schedule parameter)
   long long bytes_p1 = 0, bytes_p2 = 0;  // FP32 factor bytes read by each phase (+ dense in phase 2)
   long long multi_t_floats = 0;          // projections written by the chunk reduction
 };

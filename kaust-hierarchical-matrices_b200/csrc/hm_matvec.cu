@@ -104,7 +104,7 @@ __device__ __forceinline__ void p1_item(const LRBlock& B, int i_lo, int i_hi, co
   }
 }
 
-__global__ void __launch_bounds__(32 * kWarpsPerCta) k_p1(const P1Item* items, int nitems, const LRBlock* lr,
+__global__ void __launch_bounds__(32 * kWarpsPerCta, 3) k_p1(const P1Item* items, int nitems, const LRBlock* lr,
                                                           const float* __restrict__ X, int ldx, int nr,
                                                           float* __restrict__ T, float* __restrict__ Tpart,
                                                           int p1_rows) {

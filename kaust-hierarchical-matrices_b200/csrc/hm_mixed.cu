@@ -1,12 +1,18 @@
 // hm_mixed.cu -- mixed-precision H-matvec: BF16 hi + lo factor panels on the
 // tensor cores (mma.sync m16n8k16, FP32 accumulation).
 //
-// One product of <= 16 right-hand sides runs four kernels:
+// One product of <= 16 right-hand sides runs four or five kernels:
 //   k_mx_split_x  X (FP32, tree order) -> BF16 hi + lo fragments per 32-row tile
-//   k_mx_p1       S = panel^T X per (panel, column group, row chunk)
-//   k_mx_gather   T = S summed over row chunks, each column moved to the panel
+//   k_mx_p1       P = panel^T X per (panel, column group, row chunk); a panel
+//                 projected in one row chunk stores P, indexed by its global
+//                 column tile, else each chunk's partial
+//   k_mx_reduce   (panels of several row chunks only) the partials summed in
+//                 chunk order into P
+//   k_mx_gather   T = P with every column moved to the column of the panel
 //                 that expands it (the mirror block's factor), split hi + lo
 //   k_mx_p2       Y = sum over the ancestors' panels of U T, plus dense blocks
+// All stores are whole 16-byte fragment words; only the gather reads single
+// floats (the permutation moves whole block runs, so its reads stay local).
 // Each product of a BF16 pair uses three MMAs (hi*lo, lo*hi, hi*hi; lo*lo is
 // below FP32 rounding); the low-part MMA of a factor is skipped for the tiles
 // that carry none.  The tensor core's internal sums do not round to nearest, so
@@ -64,7 +70,8 @@ __global__ void __launch_bounds__(128) k_mx_split_x(const float* __restrict__ X,
 // row tiles.  NCT: column tiles compiled for, RU: row tiles loaded per step.
 template <int NCT, int RU>
 __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, const uint4* __restrict__ store,
-                                           const uint4* __restrict__ Xf, float4* __restrict__ S, int lane) {
+                                           const uint4* __restrict__ Xf, float4* __restrict__ S,
+                                           float4* __restrict__ Pr, int lane) {
   float acc[NCT][4];
 #pragma unroll
   for (int j = 0; j < NCT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
@@ -107,34 +114,193 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
       }
     }
   }
-  float4* out = S + (P.s0 + (long long)u.chunk * P.nct + u.ct0) * 32 + lane;
+  // the whole projection (indexed by global column tile) or one chunk's partial
+  float4* out = P.nchunk == 1 ? Pr + (P.t0 + u.ct0) * 32 + lane
+                              : S + (P.s0 + (long long)u.chunk * P.nct + u.ct0) * 32 + lane;
 #pragma unroll
   for (int j = 0; j < NCT; ++j)
     if (j < u.nct) out[j * 32] = make_float4(acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
 }
 
-__global__ void __launch_bounds__(128) k_mx_p1(const MxUnit* __restrict__ units, int nunits,
+// (three CTAs per SM: 12 warps keep enough loads in flight)
+__global__ void __launch_bounds__(128, 3) k_mx_p1(const MxUnit* __restrict__ units, int nunits,
                                                const MxPanel* __restrict__ panels, const uint4* __restrict__ store,
-                                               const uint4* __restrict__ Xf, float4* __restrict__ S) {
+                                               const uint4* __restrict__ Xf, float4* __restrict__ S,
+                                               float4* __restrict__ Pr) {
   const int w = blockIdx.x * 4 + (threadIdx.x >> 5);
   if (w >= nunits) return;
   const int lane = threadIdx.x & 31;
   const MxUnit u = units[w];
   const MxPanel P = panels[u.panel];
   if (u.nct > 4)
-    mx_p1_unit<8, 1>(u, P, store, Xf, S, lane);
+    mx_p1_unit<8, 1>(u, P, store, Xf, S, Pr, lane);
   else if (u.nct > 2)
-    mx_p1_unit<4, 2>(u, P, store, Xf, S, lane);
+    mx_p1_unit<4, 2>(u, P, store, Xf, S, Pr, lane);
   else
-    mx_p1_unit<2, 4>(u, P, store, Xf, S, lane);
+    mx_p1_unit<2, 4>(u, P, store, Xf, S, Pr, lane);
+}
+
+// ---- phase 1, persistent warps with a cp.async ring --------------------------
+// The same product as k_mx_p1.  Each warp walks its units (w, w + W, ...) one
+// row tile at a time; a step's tiles (X hi/lo fragments, the V tiles and their
+// low parts) are copied into a per-warp shared-memory ring RING - 1 steps
+// ahead of the MMAs.  In the fragment order each lane needs exactly the 16
+// bytes it copied, so every lane copies and reads its own slots: completion
+// is cp.async.wait_group on the lane's own groups, with no barrier.
+__device__ __forceinline__ void cp16(uint32_t saddr, const void* g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// WARPS per CTA, RING stages per warp, VT column tiles per unit at most
+// (slots per stage: 4 X fragments + VT high + VT low tiles).
+template <int WARPS, int RING, int VT>
+constexpr size_t ring_smem() {
+  return (size_t)WARPS * RING * (4 + 2 * VT) * 512;
+}
+
+template <int WARPS, int RING, int VT>
+__global__ void __launch_bounds__(32 * WARPS, 1) k_mx_p1r(const MxUnit* __restrict__ units, int nunits,
+                                                          const MxPanel* __restrict__ panels,
+                                                          const uint4* __restrict__ store,
+                                                          const uint4* __restrict__ Xf, float4* __restrict__ S,
+                                                          float4* __restrict__ Pr) {
+  constexpr int SLOTS = 4 + 2 * VT;
+  extern __shared__ __align__(16) uint4 ring[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int W = gridDim.x * WARPS;
+  int pu = blockIdx.x * WARPS + warp;  // producer's unit
+  if (pu >= nunits) return;            // the whole warp
+  uint4* my = ring + (size_t)warp * RING * SLOTS * 32 + lane;  // slot s of stage q: my[(q * SLOTS + s) * 32]
+  const uint32_t my_s = (uint32_t)__cvta_generic_to_shared(my);
+  MxUnit U = units[pu];
+  MxPanel PP = panels[U.panel];
+  int prt = 0;
+  auto produce = [&](int stage) {
+    if (pu < nunits) {
+      const long long rt = U.rt0 + prt;
+      const uint32_t base = my_s + (uint32_t)(stage * SLOTS * 32) * 16u;
+      const uint4* xp = Xf + (size_t)(PP.tile0 + rt) * 128 + lane;
+#pragma unroll
+      for (int p = 0; p < 4; ++p) cp16(base + (uint32_t)(p * 32) * 16u, xp + p * 32);
+      const uint4* hp = store + (PP.hi1 + rt * PP.nct + U.ct0) * 32 + lane;
+      for (int j = 0; j < U.nct; ++j) cp16(base + (uint32_t)((4 + j) * 32) * 16u, hp + j * 32);
+      const int nl = min(U.nct, max(0, PP.nctl - U.ct0));
+      const uint4* lp = store + (PP.lo1 + rt * PP.nctl + U.ct0) * 32 + lane;
+      for (int j = 0; j < nl; ++j) cp16(base + (uint32_t)((4 + VT + j) * 32) * 16u, lp + j * 32);
+      if (++prt == U.nrt) {
+        prt = 0;
+        pu += W;
+        if (pu < nunits) {
+          U = units[pu];
+          PP = panels[U.panel];
+        }
+      }
+    }
+    cp_commit();  // an empty group past the end keeps the group count uniform
+  };
+  int cu = blockIdx.x * WARPS + warp;  // consumer's unit
+  MxUnit CU = U;
+  MxPanel CP = PP;
+  int crt = 0;
+#pragma unroll
+  for (int q = 0; q < RING - 1; ++q) produce(q);
+  float acc[VT][4];
+#pragma unroll
+  for (int j = 0; j < VT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  int stage = 0;
+  while (cu < nunits) {
+    produce(stage == 0 ? RING - 1 : stage - 1);
+    cp_wait<RING - 1>();  // this lane's copies of `stage` have landed
+    const uint4* sl = my + (size_t)stage * SLOTS * 32;
+    const uint4 x0 = sl[0], x1 = sl[32], x2 = sl[64], x3 = sl[96];
+    float d[VT][4];
+#pragma unroll
+    for (int j = 0; j < VT; ++j) d[j][0] = d[j][1] = d[j][2] = d[j][3] = 0.f;
+    // the column tiles' MMA chains interleaved, so that consecutive MMAs are independent
+#pragma unroll
+    for (int j = 0; j < VT; ++j)
+      if (j < CU.nct) {
+        const uint4 vh = sl[(4 + j) * 32];
+        mma_a4(d[j], x2, vh.x, vh.y);  // X_lo V_hi
+      }
+#pragma unroll
+    for (int j = 0; j < VT; ++j)
+      if (j < CU.nct) {
+        const uint4 vh = sl[(4 + j) * 32];
+        mma_a4(d[j], x3, vh.z, vh.w);
+      }
+#pragma unroll
+    for (int j = 0; j < VT; ++j)
+      if (j < CU.nct && CU.ct0 + j < CP.nctl) {  // X_hi V_lo
+        const uint4 vl = sl[(4 + VT + j) * 32];
+        mma_a4(d[j], x0, vl.x, vl.y);
+        mma_a4(d[j], x1, vl.z, vl.w);
+      }
+#pragma unroll
+    for (int j = 0; j < VT; ++j)
+      if (j < CU.nct) {
+        const uint4 vh = sl[(4 + j) * 32];
+        mma_a4(d[j], x0, vh.x, vh.y);  // X_hi V_hi
+      }
+#pragma unroll
+    for (int j = 0; j < VT; ++j)
+      if (j < CU.nct) {
+        const uint4 vh = sl[(4 + j) * 32];
+        mma_a4(d[j], x1, vh.z, vh.w);
+        add4(acc[j], d[j]);
+      }
+    if (++crt == CU.nrt) {
+      float4* out = CP.nchunk == 1 ? Pr + (CP.t0 + CU.ct0) * 32 + lane
+                                   : S + (CP.s0 + (long long)CU.chunk * CP.nct + CU.ct0) * 32 + lane;
+#pragma unroll
+      for (int j = 0; j < VT; ++j) {
+        if (j < CU.nct) out[j * 32] = make_float4(acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+        acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+      }
+      crt = 0;
+      cu += W;
+      if (cu < nunits) {
+        CU = units[cu];
+        CP = panels[CU.panel];
+      }
+    }
+    stage = stage + 1 == RING ? 0 : stage + 1;
+  }
+  cp_wait<0>();
+}
+
+// ---- row-chunk reduction ------------------------------------------------------
+// For panels projected in several row chunks: the chunk partials of each
+// column tile summed in chunk order (deterministic) into P.
+__global__ void k_mx_reduce(const int2* __restrict__ mtiles, long long nmt, const MxPanel* __restrict__ panels,
+                            const float4* __restrict__ S, float4* __restrict__ Pr) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nmt * 32) return;
+  const int2 mt = mtiles[i >> 5];  // (panel, column tile)
+  const int lane = (int)(i & 31);
+  const MxPanel P = panels[mt.x];
+  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int ch = 0; ch < P.nchunk; ++ch) {
+    const float4 a = S[(P.s0 + (long long)ch * P.nct + mt.y) * 32 + lane];
+    v.x += a.x;
+    v.y += a.y;
+    v.z += a.z;
+    v.w += a.w;
+  }
+  Pr[(P.t0 + mt.y) * 32 + lane] = v;
 }
 
 // ---- column gather ----------------------------------------------------------
 // T tile word of lane (g,t) = {hi(T[2t][g], T[2t+1][g]), hi(.. g+8), lo(.. g), lo(.. g+8)}
-// where T[c][r] = sum over the source panel's row chunks of S[source column][r].
-// S tile: lane (g,t) = {C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1]}.
-__global__ void k_mx_gather(const int2* __restrict__ tsrc, long long t_tiles, const MxPanel* __restrict__ panels,
-                            const float* __restrict__ S, uint4* __restrict__ T) {
+// with T[c][r] = P[tinv[c]][r] (0 for padding).  P tile (C fragment): lane
+// (g,t) = {P[2t][g], P[2t+1][g], P[2t][g+8], P[2t+1][g+8]}.
+__global__ void k_mx_gather(const int* __restrict__ tinv, long long t_tiles, const float* __restrict__ Pr,
+                            uint4* __restrict__ T) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= t_tiles * 32) return;
   const long long tile = i >> 5;
@@ -142,17 +308,12 @@ __global__ void k_mx_gather(const int2* __restrict__ tsrc, long long t_tiles, co
   float v[2][2];
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
-    const int2 src = __ldg(tsrc + tile * 8 + 2 * t + c);
+    const int sc = __ldg(tinv + tile * 8 + 2 * t + c);
     float a = 0.f, b = 0.f;
-    if (src.x >= 0) {
-      const MxPanel& P = panels[src.x];
-      const int cc = src.y;
-      const long long base = (P.s0 + (cc >> 3)) * 128 + (4 * g + ((cc & 7) >> 1)) * 4 + (cc & 1);
-      const long long stride = (long long)P.nct * 128;
-      for (int ch = 0; ch < P.nchunk; ++ch) {
-        a += __ldg(S + base + ch * stride);
-        b += __ldg(S + base + ch * stride + 2);
-      }
+    if (sc >= 0) {
+      const float* p = Pr + (size_t)(sc >> 3) * 128 + (4 * g + ((sc & 7) >> 1)) * 4 + (sc & 1);
+      a = __ldg(p);
+      b = __ldg(p + 2);
     }
     v[c][0] = a;
     v[c][1] = b;
@@ -202,17 +363,38 @@ __global__ void __launch_bounds__(128) k_mx_p2(int num_tiles, int depth, const i
 #pragma unroll
     for (int nb = 0; nb < 2; ++nb) acc[mt][nb][0] = acc[mt][nb][1] = acc[mt][nb][2] = acc[mt][nb][3] = 0.f;
   const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+  // every ancestor's panel descriptor at once (lane l - 1 holds level l's),
+  // instead of a chain of dependent loads per level
+  int my_p = -1;
+  long long my_u = 0, my_l = 0, my_t = 0;
+  int my_nct = 0, my_nctl = 0;
+  if (lane < depth) {
+    const int l = lane + 1;
+    my_p = __ldg(pan_of + (1 << l) - 1 + (x >> (depth - l)));
+    if (my_p >= 0) {
+      const MxPanel P = panels[my_p];
+      const long long rt = G - P.tile0;
+      my_u = P.hi2 + rt * P.nct;
+      my_l = P.lo2 + rt * P.nctl;
+      my_t = P.t0;
+      my_nct = P.nct;
+      my_nctl = P.nctl;
+    }
+  }
   for (int l = 1; l <= depth; ++l) {
-    const int p = __ldg(pan_of + (1 << l) - 1 + (x >> (depth - l)));
+    const int p = __shfl_sync(0xffffffffu, my_p, l - 1);
     if (p < 0) continue;
-    const MxPanel P = panels[p];
-    const long long rt = G - P.tile0;
-    const uint4* uh = store + (P.hi2 + rt * P.nct) * 32 + lane;
-    const uint4* ul = store + (P.lo2 + rt * P.nctl) * 32 + lane;
-    const uint4* tt = T + P.t0 * 32 + lane;
+    const long long ou = __shfl_sync(0xffffffffu, my_u, l - 1);
+    const long long ol = __shfl_sync(0xffffffffu, my_l, l - 1);
+    const long long ot = __shfl_sync(0xffffffffu, my_t, l - 1);
+    const int nct = __shfl_sync(0xffffffffu, my_nct, l - 1);
+    const int nctl = __shfl_sync(0xffffffffu, my_nctl, l - 1);
+    const uint4* uh = store + ou * 32 + lane;
+    const uint4* ul = store + ol * 32 + lane;
+    const uint4* tt = T + ot * 32 + lane;
 #pragma unroll 2
-    for (int ct = 0; ct < P.nct; ct += 2) {
-      const bool two = ct + 1 < P.nct, lo0 = ct < P.nctl, lo1 = ct + 1 < P.nctl;
+    for (int ct = 0; ct < nct; ct += 2) {
+      const bool two = ct + 1 < nct, lo0 = ct < nctl, lo1 = ct + 1 < nctl;
       const uint4 h0 = __ldcs(uh + ct * 32);
       const uint4 h1 = two ? __ldcs(uh + (ct + 1) * 32) : z;
       const uint4 l0 = lo0 ? __ldcs(ul + ct * 32) : z;
@@ -458,7 +640,7 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
 
   // column sources and the projection's column map
   std::vector<const float*> colsrc((size_t)t_tiles * 8, nullptr);
-  std::vector<int2> tsrc((size_t)t_tiles * 8, make_int2(-1, -1));
+  std::vector<int> tinv((size_t)t_tiles * 8, -1);  // partner column (an involution)
   long long bytes_lr = 0;
   for (size_t i = 0; i < pairs.size(); ++i) {
     const MxPair& q = pairs[i];
@@ -470,8 +652,8 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
       const int cv = c < q.khi ? colL_v[i] + c : colH_v[i] + c - q.khi;
       colsrc[bu + cu] = q.fu + (size_t)c * q.m;
       colsrc[bv + cv] = q.fv + (size_t)c * q.n;
-      tsrc[bu + cu] = make_int2(pv, cv);  // Y_u += fu (fv^T X_v)
-      tsrc[bv + cv] = make_int2(pu, cu);  // Y_v += fv (fu^T X_u)
+      tinv[bv + cv] = (int)(bu + cu);  // Y_u += fu (fv^T X_v)
+      tinv[bu + cu] = (int)(bv + cv);  // Y_v += fv (fu^T X_u)
     }
     bytes_lr += 2ll * (q.m + q.n) * (q.k + q.khi);
   }
@@ -515,11 +697,12 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   M.store_tiles = tiles;
   HM_TRY(M.store.alloc((size_t)std::max<long long>(tiles, 1) * 32));
   M.h_panels = panels;
-  HM_TRY(mixed_schedule(h, M.chunk_tiles, M.group_tiles, s));
+  HM_TRY(mixed_schedule(h, M.chunk_tiles, M.group_tiles, M.p1_ring ? 1 : 0, s));
   HM_TRY(upload(M.pan_of, pan_of, s));
   HM_TRY(upload(M.tile_leaf, tile_leaf, s));
   HM_TRY(upload(M.leaf_tile0, leaf_tile0, s));
-  HM_TRY(upload(M.tsrc, tsrc, s));
+  if ((long long)t_tiles * 8 > 0x7fffffffll) return fail(HM_ERR_UNSUPPORTED, "mixed form: too many factor columns");
+  HM_TRY(upload(M.tinv, tinv, s));
   HM_TRY(upload(M.dense, dense, s));
   HM_TRY(upload(M.leaf_dptr, dptr, s));
   HM_TRY(upload(M.leaf_dblk, dblk, s));
@@ -570,18 +753,32 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   return HM_OK;
 }
 
-hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, cudaStream_t s) {
+hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, int p1_ring, cudaStream_t s) {
   MxPlan& M = h->mx;
+  if (p1_ring) {
+    int dev = 0;
+    HM_CUDA(cudaGetDevice(&dev));
+    HM_CUDA(cudaDeviceGetAttribute(&M.num_sms, cudaDevAttrMultiProcessorCount, dev));
+    HM_CUDA(cudaFuncSetAttribute(k_mx_p1r<8, 3, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ring_smem<8, 3, 4>()));
+    HM_CUDA(cudaFuncSetAttribute(k_mx_p1r<4, 4, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ring_smem<4, 4, 8>()));
+  }
+  M.p1_ring = p1_ring != 0;
   if (chunk_tiles < 1 || group_tiles < 1 || group_tiles > 8)
     return fail(HM_ERR_INVALID, "mixed schedule: need chunk >= 1 and 1 <= group <= 8 column tiles");
   std::vector<MxPanel>& panels = M.h_panels;
   long long s_tiles = 0;
   std::vector<MxUnit> units;
+  std::vector<int2> mtiles;  // column tiles of panels projected in several row chunks
   for (int p = 0; p < (int)panels.size(); ++p) {
     MxPanel& P = panels[p];
     P.nchunk = std::max(1, (P.nrt + chunk_tiles - 1) / chunk_tiles);
     P.s0 = s_tiles;
-    s_tiles += (long long)P.nchunk * P.nct;
+    if (P.nchunk > 1) {
+      s_tiles += (long long)P.nchunk * P.nct;
+      for (int c = 0; c < P.nct; ++c) mtiles.push_back(make_int2(p, c));
+    }
     for (int c = 0; c < P.nct; c += group_tiles)
       for (int ch = 0; ch < P.nchunk; ++ch)
         units.push_back(MxUnit{p, c, std::min(group_tiles, P.nct - c), ch * chunk_tiles,
@@ -592,7 +789,9 @@ hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, cuda
                    [](const MxUnit& a, const MxUnit& b) { return a.nrt * a.nct > b.nrt * b.nct; });
   HM_TRY(upload(M.panels, panels, s));
   HM_TRY(upload(M.units, units, s));
+  HM_TRY(upload(M.mtiles, mtiles, s));
   HM_CUDA(cudaStreamSynchronize(s));
+  M.nmt = (long long)mtiles.size();
   M.num_units = (int)units.size();
   M.s_tiles = s_tiles;
   M.chunk_tiles = chunk_tiles;
@@ -604,8 +803,9 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
                           cudaStream_t s, KernelMarks* km) {
   MxPlan& M = h->mx;
   uint4* Xf = reinterpret_cast<uint4*>(scratch);
-  float* S = scratch + (size_t)M.num_tiles * 4 * 128;
-  uint4* T = reinterpret_cast<uint4*>(S + (size_t)M.s_tiles * 128);
+  float4* S = reinterpret_cast<float4*>(scratch + (size_t)M.num_tiles * 4 * 128);
+  float4* Pr = S + (size_t)M.s_tiles * 32;
+  uint4* T = reinterpret_cast<uint4*>(Pr + (size_t)M.t_tiles * 32);
   const int* leaf_off = h->tree->offsets.p;
   if (M.num_tiles > 0) {
     k_mx_split_x<<<(M.num_tiles + 3) / 4, 128, 0, s>>>(X, ldx, nr, M.num_tiles, M.tile_leaf.p, M.leaf_tile0.p,
@@ -614,13 +814,26 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
     if (km) km->mark("k_mx_split_x", 4ll * h->n * nr + 4ll * h->n * 16, s);
   }
   if (M.num_units > 0) {
-    k_mx_p1<<<(M.num_units + 3) / 4, 128, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf,
-                                                  reinterpret_cast<float4*>(S));
+    if (M.p1_ring && M.group_tiles <= 4) {
+      k_mx_p1r<8, 3, 4><<<M.num_sms, 256, ring_smem<8, 3, 4>(), s>>>(M.units.p, M.num_units, M.panels.p, M.store.p,
+                                                                      Xf, S, Pr);
+    } else if (M.p1_ring) {
+      k_mx_p1r<4, 4, 8><<<M.num_sms, 128, ring_smem<4, 4, 8>(), s>>>(M.units.p, M.num_units, M.panels.p, M.store.p,
+                                                                      Xf, S, Pr);
+    } else {
+      k_mx_p1<<<(M.num_units + 3) / 4, 128, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf, S, Pr);
+    }
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_mx_p1", M.bytes_p1 + 4ll * h->n * 16, s);
   }
+  if (M.nmt > 0) {
+    k_mx_reduce<<<(unsigned)((M.nmt * 32 + 255) / 256), 256, 0, s>>>(M.mtiles.p, M.nmt, M.panels.p, S, Pr);
+    HM_LAUNCH_CHECK();
+    if (km) km->mark("k_mx_reduce", 512ll * M.s_tiles + 512ll * M.nmt, s);
+  }
   if (M.t_tiles > 0) {
-    k_mx_gather<<<(unsigned)((M.t_tiles * 32 + 255) / 256), 256, 0, s>>>(M.tsrc.p, M.t_tiles, M.panels.p, S, T);
+    k_mx_gather<<<(unsigned)((M.t_tiles * 32 + 255) / 256), 256, 0, s>>>(M.tinv.p, M.t_tiles,
+                                                                         reinterpret_cast<const float*>(Pr), T);
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_mx_gather", 2ll * h->stats.rank_sum * 16 * 4, s);
   }

@@ -65,16 +65,22 @@ struct MxPlan {
   DevBuf<int> tile_leaf;   // global row tile -> leaf
   DevBuf<int> leaf_tile0;  // leaf -> first global row tile (num_leaves + 1)
   int num_tiles = 0;
-  DevBuf<int2> tsrc;       // phase-2 column (8 * t0 + c) -> (source panel, source column) or (-1, -1)
+  DevBuf<int> tinv;        // global factor column (8 * t0 + c) -> its mirror column, or -1 (padding)
+  DevBuf<int2> mtiles;     // (panel, column tile) of panels projected in several row chunks
+  long long nmt = 0;
   long long s_tiles = 0, t_tiles = 0;
   DevBuf<MxDense> dense;
   int num_dense = 0;
   DevBuf<int> leaf_dptr, leaf_dblk;  // dense blocks covering each leaf's rows
   long long bytes_p1 = 0, bytes_p2 = 0;  // BF16 bytes of the factors (unpadded) and dense blocks
   std::vector<MxPanel> h_panels;          // host copy (the schedule rebuilds units and S offsets)
-  int chunk_tiles = 64, group_tiles = 8;  // phase-1 unit shape (schedule parameters)
-  // scratch of one 16-column panel of right-hand sides, in floats
-  long long scratch_floats() const { return ((long long)num_tiles * 4 + s_tiles + t_tiles) * 128; }
+  int chunk_tiles = 128, group_tiles = 4;  // phase-1 unit shape (schedule parameters)
+  bool p1_ring = false;                    // phase 1 by persistent warps with a cp.async ring
+  int num_sms = 148;
+  // scratch of one 16-column panel of right-hand sides, in floats: X
+  // fragments, chunk partials, projections P (by source column), T (by
+  // expanding column, BF16 hi + lo)
+  long long scratch_floats() const { return ((long long)num_tiles * 4 + s_tiles + 2 * t_tiles) * 128; }
 };
 
 struct MxPair {  // one stored low-rank pair (u rows, v columns) = fu fv^T, and its mirror
@@ -96,9 +102,10 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
 struct KernelMarks;
 
 // Phase-1 units of chunk_tiles row tiles x group_tiles (<= 8) column tiles,
-// and the projection's S layout that goes with them.  The caller rebuilds the
+// the projection's S layout that goes with them, and the phase-1 kernel
+// (p1_ring: persistent warps with a cp.async ring, else one warp per unit).  The caller rebuilds the
 // matvec plan afterwards (the scratch size changes).
-hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, cudaStream_t s);
+hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, int p1_ring, cudaStream_t s);
 
 // One panel of nr <= 16 right-hand sides in tree order; scratch holds
 // scratch_floats() floats.  km (optional) receives an event after each kernel.

@@ -108,6 +108,7 @@ def lib():
             L.hm_batch_matvec.argtypes = [P, I, P, I, P, I, I, P]
             L.hm_batch_free.argtypes = [P]
             L.hm_autotune.argtypes = [P, I, ctypes.c_char_p, P, P, ctypes.c_char_p, I]
+            L.hm_schedule_set.argtypes = [P, ctypes.c_char_p, P]
         _lib = L
     return _lib
 
@@ -375,6 +376,11 @@ def autotune(H, nrhs=16, cache_path=None, stream=None):
     _check(lib().hm_autotune(H.h, nrhs, cache_path.encode() if cache_path else None, _stream(stream),
                              ctypes.byref(fc), buf, 128))
     return buf.value.decode(), bool(fc.value)
+
+
+def schedule_set(H, choice, stream=None):
+    """Apply a schedule in hm_autotune's notation (hm_schedule_set)."""
+    _check(lib().hm_schedule_set(H.h, choice.encode(), _stream(stream)))
 
 
 def default_opts(d):
