@@ -231,11 +231,13 @@ struct KmmFastArgs {
   float dscale;  // derivative factor
   int deriv;     // entries of dK/dl instead of K
   int bs, round;
-  const uint32_t* om2;      // sampling: Gaussian pairs [jp][bs8]
-  int ld_om;                // bs8
-  const uint32_t* qh;       // projection: Q pairs [jp][kpad8], hi and lo, per problem
-  const uint32_t* ql;
-  const long long* qpoff;   // per problem (batch index), words
+  // right-hand operand tables in fragment order: word (k-step, column tile,
+  // lane (g,t)) holds the m16n8k16 B fragment {b0, b1} with
+  // b0 = {W[16 ks + 2t][8 nt + g], W[16 ks + 2t + 1][..]}, b1 = rows + 8
+  const uint2* om;          // sampling: the Gaussian table, om_nt column tiles
+  int om_nt;
+  const uint4* qt;          // projection: {hi b0, hi b1, lo b0, lo b1} of Q, per problem
+  const long long* qpoff;   // per problem (batch index), 16-byte words
   int col0;                 // projection: first basis column of this launch
   float* ws;
 };
@@ -302,32 +304,36 @@ __global__ void __launch_bounds__(128) k_kmm_fast(KmmFastArgs a) {
     rcb[k] = rb_ok ? a.pts[(size_t)k * a.npts + rbase + rb] * a.scale : 0.f;
   }
   const int ntiles = min(NT, (s + 7) >> 3);
-  const uint32_t* Bh = MODE ? a.qh + a.qpoff[it.x] + col0 : a.om2;
-  const uint32_t* Bl = MODE ? a.ql + a.qpoff[it.x] + col0 : nullptr;
-  const size_t ldb = MODE ? (size_t)((S.k + 7) & ~7) : (size_t)a.ld_om;
+  const int tnt = MODE ? (S.k + 7) >> 3 : a.om_nt;  // column tiles of the table
+  const uint4* qt = MODE ? a.qt + a.qpoff[it.x] + (col0 >> 3) * 32 + lane : nullptr;
+  const uint2* om = MODE ? nullptr : a.om + lane;
   float acc[NT][4];
 #pragma unroll
   for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
   float nrm = 0.f;
   const bool want_norm = MODE == 0 && a.round == 0;
-  // B fragments of k-step kg (16 columns): rows (8 kg + t) and (8 kg + t + 4) of the pair table
+  // B fragments of k-step kg (16 columns of the block): one word per lane and column tile
   uint32_t bh[NT][2], bl[NT][2];
   auto load_b = [&](int kg) {
-    const size_t w = (size_t)(8 * kg + t) * ldb + g;
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt) {
       if (nt < ntiles) {
-        bh[nt][0] = __ldg(Bh + w + nt * 8);
-        bh[nt][1] = __ldg(Bh + w + 4 * ldb + nt * 8);
         if (MODE == 1) {
-          bl[nt][0] = __ldg(Bl + w + nt * 8);
-          bl[nt][1] = __ldg(Bl + w + 4 * ldb + nt * 8);
+          const uint4 v = __ldg(qt + ((size_t)kg * tnt + nt) * 32);
+          bh[nt][0] = v.x;
+          bh[nt][1] = v.y;
+          bl[nt][0] = v.z;
+          bl[nt][1] = v.w;
+        } else {
+          const uint2 v = __ldg(om + ((size_t)kg * tnt + nt) * 32);
+          bh[nt][0] = v.x;
+          bh[nt][1] = v.y;
         }
       }
     }
   };
   const int nks = (nc + 15) >> 4;
-  load_b(0);
+  if (MODE == 0) load_b(0);
   for (int kg = 0; kg < nks; ++kg) {
     const int c0 = (kg * 16) / kCC * kCC;
     if (kg * 16 == c0) {  // first k-step of a coordinate chunk
@@ -339,16 +345,16 @@ __global__ void __launch_bounds__(128) k_kmm_fast(KmmFastArgs a) {
       __syncthreads();
     }
     uint32_t ch[NT][2], cl[NT][2];
+    if (MODE == 1) {
+      load_b(kg);  // issued before the entries are generated, used after (no second register set)
+    } else {
 #pragma unroll
-    for (int nt = 0; nt < NT; ++nt) {
-      ch[nt][0] = bh[nt][0];
-      ch[nt][1] = bh[nt][1];
-      if (MODE == 1) {
-        cl[nt][0] = bl[nt][0];
-        cl[nt][1] = bl[nt][1];
+      for (int nt = 0; nt < NT; ++nt) {
+        ch[nt][0] = bh[nt][0];
+        ch[nt][1] = bh[nt][1];
       }
+      if (kg + 1 < nks) load_b(kg + 1);  // in flight while this k-step's entries are generated
     }
-    if (kg + 1 < nks) load_b(kg + 1);  // in flight while this k-step's entries are generated
     const int cb = kg * 16 - c0 + 2 * t;  // chunk columns cb, cb+1, cb+8, cb+9
     float e[8];
 #pragma unroll
@@ -381,9 +387,10 @@ __global__ void __launch_bounds__(128) k_kmm_fast(KmmFastArgs a) {
     for (int nt = 0; nt < NT; ++nt) {
       if (nt < ntiles) {
         float d[4] = {0.f, 0.f, 0.f, 0.f};
-        if (MODE == 1) mma_bf16(d, ah[0], ah[1], ah[2], ah[3], cl[nt][0], cl[nt][1]);
-        mma_bf16(d, al[0], al[1], al[2], al[3], ch[nt][0], ch[nt][1]);
-        mma_bf16(d, ah[0], ah[1], ah[2], ah[3], ch[nt][0], ch[nt][1]);
+        const uint32_t b0 = MODE == 1 ? bh[nt][0] : ch[nt][0], b1 = MODE == 1 ? bh[nt][1] : ch[nt][1];
+        if (MODE == 1) mma_bf16(d, ah[0], ah[1], ah[2], ah[3], bl[nt][0], bl[nt][1]);
+        mma_bf16(d, al[0], al[1], al[2], al[3], b0, b1);
+        mma_bf16(d, ah[0], ah[1], ah[2], ah[3], b0, b1);
         add4(acc[nt], d);
       }
     }
@@ -412,40 +419,54 @@ __global__ void __launch_bounds__(128) k_kmm_fast(KmmFastArgs a) {
   }
 }
 
-// Gaussian table of one sampling round in BF16 pairs: om2[jp][c] =
-// {W[2jp][c], W[2jp+1][c]} with W[j][c] the BF16-rounded N(0,1) value of
-// k_omega (columns c >= bs are zero).
-__global__ void k_omega_pack(uint32_t* om2, int rows2, int bs, int bs8, uint32_t seed, int round) {
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)rows2 * bs8;
+// Gaussian table of one sampling round in fragment order (see KmmFastArgs):
+// W[j][c] is the BF16-rounded N(0,1) value for (round, j, c), zero for c >= bs.
+__global__ void k_omega_pack(uint2* om, int ksteps, int bs, int nt_tot, uint32_t seed, int round) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)ksteps * nt_tot * 32;
        e += (long long)gridDim.x * blockDim.x) {
-    const int jp = (int)(e / bs8), c = (int)(e % bs8);
-    float x0 = 0.f, x1 = 0.f;
+    const int lane = (int)(e & 31), g = lane >> 2, t = lane & 3;
+    const long long w = e >> 5;
+    const int nt = (int)(w % nt_tot), ks = (int)(w / nt_tot);
+    const int c = nt * 8 + g, j = ks * 16 + 2 * t;
+    float x[4] = {0.f, 0.f, 0.f, 0.f};
     if (c < bs) {
-      x0 = gauss_at(seed, 0x51ed270bu + round, (uint32_t)(2 * jp), (uint32_t)c);
-      x1 = gauss_at(seed, 0x51ed270bu + round, (uint32_t)(2 * jp + 1), (uint32_t)c);
+      const uint32_t st = 0x51ed270bu + round;
+      x[0] = gauss_at(seed, st, (uint32_t)j, (uint32_t)c);
+      x[1] = gauss_at(seed, st, (uint32_t)(j + 1), (uint32_t)c);
+      x[2] = gauss_at(seed, st, (uint32_t)(j + 8), (uint32_t)c);
+      x[3] = gauss_at(seed, st, (uint32_t)(j + 9), (uint32_t)c);
     }
-    om2[e] = pack_bf16(x0, x1);
+    om[e] = make_uint2(pack_bf16(x[0], x[1]), pack_bf16(x[2], x[3]));
   }
 }
 
-// Q (m x k, column-major, ld m) of each problem -> BF16 pairs along rows,
-// hi and lo: word (jp, c) = {Q[2jp][c], Q[2jp+1][c]}, jp < mpad/2, c < kpad8.
+// Q (m x k, column-major, ld m) of each problem in fragment order, hi and lo
+// (see KmmFastArgs): k-steps over the rows padded to whole coordinate chunks,
+// column tiles over k padded to 8.
 __global__ void k_pack_q(const Prob* probs, const ProbState* st, const float* ws, const long long* qpoff,
-                         uint32_t* qh, uint32_t* ql) {
+                         uint4* qt) {
   const Prob P = probs[blockIdx.x];
   const int k = st[blockIdx.x].k;
   if (k <= 0) return;
-  const int kp = (k + 7) & ~7;
-  const int rows2 = (P.m + kCC - 1) / kCC * (kCC / 2);
+  const int ntq = (k + 7) >> 3;
+  const int ksteps = (P.m + kCC - 1) / kCC * (kCC / 16);
   const float* Q = ws + P.qoff;
-  uint32_t* h = qh + qpoff[blockIdx.x];
-  uint32_t* l = ql + qpoff[blockIdx.x];
-  for (int e = threadIdx.x; e < rows2 * kp; e += blockDim.x) {
-    const int jp = e / kp, c = e % kp;
-    const int i0 = 2 * jp;
-    const float x0 = (c < k && i0 < P.m) ? Q[(size_t)c * P.m + i0] : 0.f;
-    const float x1 = (c < k && i0 + 1 < P.m) ? Q[(size_t)c * P.m + i0 + 1] : 0.f;
-    split_bf16x2(x0, x1, h[e], l[e]);
+  uint4* q = qt + qpoff[blockIdx.x];
+  for (int e = threadIdx.x; e < ksteps * ntq * 32; e += blockDim.x) {
+    const int lane = e & 31, g = lane >> 2, t = lane & 3;
+    const int w = e >> 5;
+    const int nt = w % ntq, ks = w / ntq;
+    const int c = nt * 8 + g, i = ks * 16 + 2 * t;
+    float x[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int row = i + (r & 1) + 8 * (r >> 1);
+      x[r] = (c < k && row < P.m) ? Q[(size_t)c * P.m + row] : 0.f;
+    }
+    uint4 o;
+    split_bf16x2(x[0], x[1], o.x, o.z);
+    split_bf16x2(x[2], x[3], o.y, o.w);
+    q[e] = o;
   }
 }
 
@@ -1221,7 +1242,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       constexpr bool kTensor = std::is_same<W, float>::value;
       const bool fast = kTensor && t->d <= 3;
       KmmFastArgs kf{};
-      DevBuf<uint32_t> om2;
+      DevBuf<uint2> om2;
       int bs0 = bs_first;  // first round's sample width
       for (const Prob& P : bp)
         if (P.kmax < bs0) bs0 = bs;
@@ -1230,8 +1251,8 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       if (fast) {
         int max_n = 1;
         for (const Prob& P : bp) max_n = std::max(max_n, P.n);
-        om_rows2 = (max_n + kCC - 1) / kCC * (kCC / 2);
-        if ((st = om2.alloc_async((size_t)om_rows2 * bs8, stream))) return st;
+        om_rows2 = (max_n + kCC - 1) / kCC * (kCC / 2);  // column pairs; k-steps = om_rows2 / 8
+        if ((st = om2.alloc_async((size_t)(om_rows2 / 8) * (bs8 / 8) * 32, stream))) return st;
         const double il = 1.0 / opt.ell, log2e = 1.4426950408889634, ln2 = 0.6931471805599453;
         double sc = log2e * il, dsc = ln2 * il;
         if (opt.kernel == HM_KERNEL_MATERN32) {
@@ -1249,8 +1270,8 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
         kf.dscale = (float)dsc;
         kf.deriv = opt.derivative != 0;
         kf.bs = bs;
-        kf.om2 = om2.p;
-        kf.ld_om = bs8;
+        kf.om = om2.p;
+        kf.om_nt = bs8 / 8;
         kf.ws = reinterpret_cast<float*>(ws.p);
       }
       tr.mark("batch setup", stream, nb);
@@ -1258,7 +1279,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       for (int round = 0; round < max_rounds; ++round) {
         if (fast) {
           const int rbs = round == 0 ? bs0 : bs;
-          k_omega_pack<<<592, 256, 0, stream>>>(om2.p, om_rows2, rbs, bs8, ka.seed, round);
+          k_omega_pack<<<592, 256, 0, stream>>>(om2.p, om_rows2 / 8, rbs, bs8 / 8, ka.seed, round);
           HM_LAUNCH_CHECK();
           kf.round = round;
           kf.bs = rbs;
@@ -1284,7 +1305,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       }
       tr.mark("sample rounds", stream, nb);
       // B = A^T Q
-      DevBuf<uint32_t> qh, ql;
+      DevBuf<uint4> qt;
       DevBuf<long long> dqpoff;
       DevBuf<int2> dcls;
       if (fast) {
@@ -1292,17 +1313,15 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
         size_t qw = 0;
         for (int i = 0; i < nb; ++i) {
           qpoff[i] = (long long)qw;
-          if (hst[i].k > 0) qw += (size_t)(bp[i].m + kCC - 1) / kCC * (kCC / 2) * (size_t)((hst[i].k + 7) & ~7);
+          if (hst[i].k > 0)
+            qw += (size_t)(bp[i].m + kCC - 1) / kCC * (kCC / 16) * (size_t)((hst[i].k + 7) >> 3) * 32;
         }
-        if ((st = qh.alloc_async(std::max<size_t>(qw, 1), stream)) ||
-            (st = ql.alloc_async(std::max<size_t>(qw, 1), stream)) || (st = dqpoff.alloc_async(nb, stream)))
+        if ((st = qt.alloc_async(std::max<size_t>(qw, 1), stream)) || (st = dqpoff.alloc_async(nb, stream)))
           return st;
         HM_CUDA(cudaMemcpyAsync(dqpoff.p, qpoff.data(), sizeof(long long) * nb, cudaMemcpyHostToDevice, stream));
-        k_pack_q<<<nb, 256, 0, stream>>>(dprobs.p, dst.p, reinterpret_cast<const float*>(ws.p), dqpoff.p, qh.p,
-                                         ql.p);
+        k_pack_q<<<nb, 256, 0, stream>>>(dprobs.p, dst.p, reinterpret_cast<const float*>(ws.p), dqpoff.p, qt.p);
         HM_LAUNCH_CHECK();
-        kf.qh = qh.p;
-        kf.ql = ql.p;
+        kf.qt = qt.p;
         kf.qpoff = dqpoff.p;
         // one launch per basis-width class, so the narrow (most) blocks run
         // with few accumulator registers
