@@ -47,7 +47,14 @@ constexpr int kOrthThreads = 256;
 constexpr int kMaxCols = 256;  // max basis columns of one block (rank cap)
 constexpr int kTruncMax = 128; // widest basis the SVD truncation handles (wider: kept as sampled)
 constexpr int kColGroup = 128; // projection columns per sketch launch
-constexpr int kMaxBs = 32;     // max sample block
+constexpr int kMaxBs = 32;     // max sample block (the option)
+// widest sample (basis + test columns) one orthogonalisation handles; the
+// shared memory and per-thread arrays of k_orth scale with it (64 halves the
+// CTAs per SM, measured slower while the sample stays at 32 columns)
+template <typename W>
+constexpr int max_bs() {
+  return 32;
+}
 
 struct Prob {
   int r0, m, c0, n;
@@ -344,7 +351,7 @@ __global__ void __launch_bounds__(128) k_kmm_fast(KmmFastArgs a) {
       }
       __syncthreads();
     }
-    uint32_t ch[NT][2], cl[NT][2];
+    uint32_t ch[NT][2];
     if (MODE == 1) {
       load_b(kg);  // issued before the entries are generated, used after (no second register set)
     } else {
@@ -477,8 +484,10 @@ void launch_kmm_fast3(int mode, int nt, unsigned grid, cudaStream_t s, const Kmm
   if (mode == 0) {
     if (nt <= 2)
       k_kmm_fast<D, KIND, 0, 2><<<grid, 128, 0, s>>>(a);
+    else if (nt <= 4)
+      k_kmm_fast<D, KIND, 0, 4><<<grid, 128, 0, s>>>(a);
     else
-      k_kmm_fast<D, KIND, 0, kMaxBs / 8><<<grid, 128, 0, s>>>(a);
+      k_kmm_fast<D, KIND, 0, 8><<<grid, 128, 0, s>>>(a);
   } else {
     if (nt <= 4)
       k_kmm_fast<D, KIND, 1, 4><<<grid, 128, 0, s>>>(a);
@@ -514,7 +523,8 @@ struct OrthArgs {
   const Prob* probs;
   ProbState* st;
   W* ws;
-  int bs;
+  int bs;          // sample columns of this round
+  int bst;         // of which the last bst are test columns (0: none)
   double thresh2;  // stop when est <= thresh2 * normA2
   int round;
 };
@@ -523,12 +533,12 @@ struct OrthArgs {
 template <typename W>
 __device__ void block_qty(const W* Q, const W* Y, int m, int k, int bs, W* Csm, W* stage) {
   const int t = threadIdx.x;
-  constexpr int kPer = kMaxCols * kMaxBs / kOrthThreads;  // outputs per thread
+  constexpr int kPer = kMaxCols * max_bs<W>() / kOrthThreads;  // outputs per thread
   W accv[kPer];
 #pragma unroll
   for (int i = 0; i < kPer; ++i) accv[i] = W(0);
   W* Qs = stage;                  // [kMaxCols][33]
-  W* Ys = stage + kMaxCols * 33;  // [kMaxBs][33]
+  W* Ys = stage + kMaxCols * 33;  // [max_bs][33]
   const int nout = k * bs;
   for (int i0 = 0; i0 < m; i0 += 32) {
     for (int e = t; e < 32 * k; e += kOrthThreads) {
@@ -564,7 +574,7 @@ __device__ void block_qty(const W* Q, const W* Y, int m, int k, int bs, W* Csm, 
 template <typename W>
 __device__ void block_update(const W* Q, W* Y, int m, int k, int bs, const W* Csm) {
   for (int i = threadIdx.x; i < m; i += kOrthThreads) {
-    W y[kMaxBs];
+    W y[max_bs<W>()];
     for (int c = 0; c < bs; ++c) y[c] = Y[(size_t)c * m + i];
     for (int j = 0; j < k; ++j) {
       W qv = Q[(size_t)j * m + i];
@@ -579,8 +589,11 @@ __device__ void block_update(const W* Q, W* Y, int m, int k, int bs, const W* Cs
 template <typename W>
 __device__ void gram64(const W* Y, int m, int cols, double* Gs, W* stage) {
   const int t = threadIdx.x;
-  double accv[4] = {0, 0, 0, 0};
-  W* Ys = stage;  // [kMaxBs][33]
+  constexpr int kPer = max_bs<W>() * max_bs<W>() / kOrthThreads;  // outputs per thread
+  double accv[kPer];
+#pragma unroll
+  for (int x = 0; x < kPer; ++x) accv[x] = 0.0;
+  W* Ys = stage;  // [max_bs][33]
   const int nout = cols * cols;
   for (int i0 = 0; i0 < m; i0 += 32) {
     for (int e = t; e < 32 * cols; e += kOrthThreads) {
@@ -589,7 +602,7 @@ __device__ void gram64(const W* Y, int m, int cols, double* Gs, W* stage) {
     }
     __syncthreads();
 #pragma unroll
-    for (int x = 0; x < 4; ++x) {
+    for (int x = 0; x < kPer; ++x) {
       int o = t + x * kOrthThreads;
       if (o < nout) {
         int a = o / cols, b = o % cols;
@@ -601,7 +614,7 @@ __device__ void gram64(const W* Y, int m, int cols, double* Gs, W* stage) {
     __syncthreads();
   }
 #pragma unroll
-  for (int x = 0; x < 4; ++x) {
+  for (int x = 0; x < kPer; ++x) {
     int o = t + x * kOrthThreads;
     if (o < nout) Gs[o] = accv[x];
   }
@@ -655,9 +668,9 @@ __device__ int chol_pivoted(double* G, int cols, int* perm, bool pivot, double t
 template <typename W>
 __device__ void apply_linv(W* Y, int m, int cols, const double* L, const int* perm, int r) {
   for (int i = threadIdx.x; i < m; i += kOrthThreads) {
-    W y[kMaxBs];
+    W y[max_bs<W>()];
     for (int c = 0; c < cols; ++c) y[c] = Y[(size_t)c * m + i];
-    double x[kMaxBs];
+    double x[max_bs<W>()];
     for (int a = 0; a < r; ++a) {
       double v = y[perm[a]];
       for (int b = 0; b < a; ++b) v -= L[a * cols + b] * x[b];
@@ -668,13 +681,67 @@ __device__ void apply_linv(W* Y, int m, int cols, const double* L, const int* pe
   __syncthreads();
 }
 
+// Orthonormalises the `cols` columns of Y (already projected against Q[0..k))
+// in place: pivoted Cholesky-QR, then two Cholesky-QR refinements; R^{-1} of
+// an ill-conditioned sample magnifies whatever the Gram-Schmidt left along
+// the old basis, so after the first refinement the block is projected against
+// Q once more.  Returns the rank r; Y[0..r) is the new orthonormal block.
+template <typename W>
+__device__ int cholqr_block(const W* Q, int k, W* Y, int m, int cols, double* Gs, int* perm, int* rank_sh,
+                            W* Csm, W* stage) {
+  gram64(Y, m, cols, Gs, stage);
+  if (threadIdx.x == 0) {
+    double tr = 0;
+    for (int c = 0; c < cols; ++c) tr += Gs[c * cols + c];
+    // columns whose norm is below FP32 resolution of the sample are noise
+    *rank_sh = chol_pivoted(Gs, cols, perm, true, 1e-10 * tr);
+  }
+  __syncthreads();
+  int r = *rank_sh;
+  if (r == 0) return 0;
+  apply_linv(Y, m, cols, Gs, perm, r);
+  for (int pass = 0; pass < 2 && r > 0; ++pass) {
+    if (pass == 1 && k > 0) {
+      block_qty(Q, Y, m, k, r, Csm, stage);
+      block_update(Q, Y, m, k, r, Csm);
+    }
+    const int rg = r;  // dimension (and row stride) of this Gram matrix
+    gram64(Y, m, rg, Gs, stage);
+    if (threadIdx.x == 0) *rank_sh = chol_pivoted(Gs, rg, perm, pass == 1, pass == 1 ? 1e-12 * rg : 0.0);
+    __syncthreads();
+    r = *rank_sh;  // a refinement that loses rank keeps the leading columns
+    if (r > 0) apply_linv(Y, m, rg, Gs, perm, r);
+  }
+  return r;
+}
+
+template <typename W>
+__device__ double trace_gram(const W* Y, int m, int cols, double* Gs, W* stage) {
+  gram64(Y, m, cols, Gs, stage);
+  double tr = 0;
+  for (int c = 0; c < cols; ++c) tr += Gs[c * cols + c];
+  return tr;
+}
+
+// One ARA round of one block.  The sample Y (m x bs) holds bs - bst basis
+// columns and bst test columns (bst = 0: every column is a basis column and
+// the estimate comes from the whole sample, as in the reference's ARA).
+//  1. the whole sample is projected against Q (classical Gram-Schmidt, twice);
+//  2. the test columns' projected norm estimates the residual
+//     ||(I - QQ^T) A||_F^2 ~ ||Y_t'||^2 / bst: below the threshold, done;
+//  3. the basis columns are orthonormalised and appended to Q;
+//  4. the test columns, projected against the new columns as well, estimate
+//     the residual left by the grown basis: below the threshold, done in this
+//     round (no extra pass); otherwise they are a sample of that residual and
+//     are orthonormalised and appended too.
 template <typename W>
 __global__ void __launch_bounds__(kOrthThreads) k_orth(OrthArgs<W> a) {
+  constexpr int MB = max_bs<W>();
   extern __shared__ __align__(16) unsigned char osm[];
-  double* Gs = reinterpret_cast<double*>(osm);              // [kMaxBs*kMaxBs]
-  W* Csm = reinterpret_cast<W*>(Gs + kMaxBs * kMaxBs);      // [kMaxCols*kMaxBs]
-  W* stage = Csm + kMaxCols * kMaxBs;                       // (kMaxCols+kMaxBs)*33
-  __shared__ int perm[kMaxBs];
+  double* Gs = reinterpret_cast<double*>(osm);         // [MB*MB]
+  W* Csm = reinterpret_cast<W*>(Gs + MB * MB);         // [kMaxCols*MB]
+  W* stage = Csm + kMaxCols * MB;                      // (kMaxCols+MB)*33
+  __shared__ int perm[MB];
   __shared__ int rank_sh;
   __shared__ int decision;  // 0 continue, 1 converged, 2 cap reached
 
@@ -682,31 +749,28 @@ __global__ void __launch_bounds__(kOrthThreads) k_orth(OrthArgs<W> a) {
   ProbState S = a.st[p];
   if (!S.active) return;
   const Prob P = a.probs[p];
-  const int m = P.m, bs = a.bs;
+  const int m = P.m, bs = a.bs, bst = a.bst, bsb = bs - bst;
   W* Q = a.ws + P.qoff;
   W* Y = a.ws + P.yoff;
+  W* Yt = Y + (size_t)bsb * m;
   int k = S.k;
   for (int pass = 0; pass < 2 && k > 0; ++pass) {
     block_qty(Q, Y, m, k, bs, Csm, stage);
     block_update(Q, Y, m, k, bs, Csm);
   }
-  gram64(Y, m, bs, Gs, stage);
-  if (threadIdx.x == 0) {
-    double tr = 0;
-    for (int c = 0; c < bs; ++c) tr += Gs[c * bs + c];
-    double est = tr / bs;
-    S.est = est;
-    S.rounds += 1;
-    if (est <= a.thresh2 * S.normA2 || S.normA2 == 0.0) decision = 1;
-    else if (k + bs > P.kmax) decision = 2;
-    else decision = 0;
-    if (decision == 0) {
-      // columns whose norm is below FP32 resolution of the sample are noise
-      double tau = 1e-10 * tr;
-      rank_sh = chol_pivoted(Gs, bs, perm, true, tau);
+  {
+    const int ne = bst > 0 ? bst : bs;
+    const double tr = trace_gram(bst > 0 ? Yt : Y, m, ne, Gs, stage);
+    if (threadIdx.x == 0) {
+      const double est = tr / ne;
+      S.est = est;
+      S.rounds += 1;
+      if (est <= a.thresh2 * S.normA2 || S.normA2 == 0.0) decision = 1;
+      else if (k + bsb > P.kmax) decision = 2;
+      else decision = 0;
     }
+    __syncthreads();
   }
-  __syncthreads();
   if (decision != 0) {
     if (threadIdx.x == 0) {
       S.active = 0;
@@ -715,38 +779,37 @@ __global__ void __launch_bounds__(kOrthThreads) k_orth(OrthArgs<W> a) {
     }
     return;
   }
-  int r = rank_sh;
-  if (r == 0) {
-    if (threadIdx.x == 0) {
-      S.active = 0;
-      S.converged = 1;
-      a.st[p] = S;
-    }
-    return;
-  }
-  apply_linv(Y, m, bs, Gs, perm, r);
-  // Refinements.  R^{-1} of an ill-conditioned sample magnifies whatever the
-  // Gram-Schmidt left along the old basis, so after the first refinement the
-  // block is projected against Q once more before the final Cholesky-QR.
-  for (int pass = 0; pass < 2 && r > 0; ++pass) {
-    if (pass == 1 && k > 0) {
-      block_qty(Q, Y, m, k, r, Csm, stage);
-      block_update(Q, Y, m, k, r, Csm);
-    }
-    const int rg = r;  // dimension (and row stride) of this Gram matrix
-    gram64(Y, m, rg, Gs, stage);
-    if (threadIdx.x == 0) rank_sh = chol_pivoted(Gs, rg, perm, pass == 1, pass == 1 ? 1e-12 * rg : 0.0);
-    __syncthreads();
-    r = rank_sh;  // a refinement that loses rank keeps the leading columns
-    if (r > 0) apply_linv(Y, m, rg, Gs, perm, r);
-  }
-  // append to Q
+  int r = cholqr_block(Q, k, Y, m, bsb, Gs, perm, &rank_sh, Csm, stage);
   for (int c = 0; c < r; ++c)
     for (int i = threadIdx.x; i < m; i += kOrthThreads) Q[(size_t)(k + c) * m + i] = Y[(size_t)c * m + i];
   __syncthreads();
+  k += r;
+  bool conv = false;
+  if (bst > 0) {
+    if (r > 0) {
+      const W* Qn = Q + (size_t)(k - r) * m;
+      for (int pass = 0; pass < 2; ++pass) {
+        block_qty(Qn, Yt, m, r, bst, Csm, stage);
+        block_update(Qn, Yt, m, r, bst, Csm);
+      }
+    }
+    const double tr = trace_gram(Yt, m, bst, Gs, stage);
+    if (threadIdx.x == 0) S.est = tr / bst;
+    conv = tr / bst <= a.thresh2 * S.normA2;
+    if (!conv && k < P.kmax) {
+      int rt = cholqr_block(Q, k, Yt, m, bst, Gs, perm, &rank_sh, Csm, stage);
+      rt = min(rt, P.kmax - k);
+      for (int c = 0; c < rt; ++c)
+        for (int i = threadIdx.x; i < m; i += kOrthThreads) Q[(size_t)(k + c) * m + i] = Yt[(size_t)c * m + i];
+      __syncthreads();
+      k += rt;
+    }
+  } else {
+    conv = r == 0;
+  }
   if (threadIdx.x == 0) {
-    S.k = k + r;
-    if (r == 0) {
+    S.k = k;
+    if (conv) {
       S.active = 0;
       S.converged = 1;
     }
@@ -1056,7 +1119,8 @@ size_t kmm_smem() {
 
 template <typename W>
 size_t orth_smem() {
-  return sizeof(double) * kMaxBs * kMaxBs + sizeof(W) * kMaxCols * kMaxBs + sizeof(W) * (kMaxCols + kMaxBs) * 33;
+  constexpr int MB = max_bs<W>();
+  return sizeof(double) * MB * MB + sizeof(W) * kMaxCols * MB + sizeof(W) * (kMaxCols + MB) * 33;
 }
 
 }  // namespace
@@ -1160,8 +1224,14 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
     // The specialised sketch kernels draw a double-width first sample (the
     // generation of the kernel block, not its product with the sample, is
     // the cost of a pass, so blocks of rank bs..2 bs finish a pass earlier).
+    // Separate test columns (k_orth's bst) are supported but measured slower
+    // on the 2^20-point Matern build (wider first passes, wider bases), so
+    // rounds use bst = 0, the reference ARA's estimate from the sample itself.
     constexpr bool kTensorW = std::is_same<W, float>::value;
-    const int bs_first = (kTensorW && t->d <= 3) ? std::min(2 * bs, kMaxBs) : bs;
+    const bool fastW = kTensorW && t->d <= 3;
+    const int bst = 0;
+    const int bs_first = fastW ? std::min(2 * bs, kMaxBs) : bs;  // round 0 basis columns
+    const int wmax = std::max(bs_first, bs) + bst;                // widest sample
     // greedy batches under the workspace budget; one workspace for all of them
     std::vector<long long> batch_end;
     size_t ws_max = 1;
@@ -1170,7 +1240,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       size_t wsz = 0;
       while (pe < nprob) {
         const Prob& P = probs[pe];
-        size_t need = (size_t)P.m * (P.kmax + bs_first) + (size_t)P.m * bs_first + (size_t)P.n * (P.kmax + bs_first);
+        size_t need = (size_t)P.m * (P.kmax + wmax) + (size_t)P.m * wmax + (size_t)P.n * (P.kmax + wmax);
         if (pe > ps && wsz + need > budget_elems) break;
         wsz += need;
         ++pe;
@@ -1194,11 +1264,11 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       for (int i = 0; i < nb; ++i) {
         Prob& P = bp[i];
         P.qoff = (long long)off;
-        off += (size_t)P.m * (P.kmax + bs_first);
+        off += (size_t)P.m * (P.kmax + wmax);
         P.yoff = (long long)off;
-        off += (size_t)P.m * bs_first;
+        off += (size_t)P.m * wmax;
         P.boff = (long long)off;
-        off += (size_t)P.n * (P.kmax + bs_first);
+        off += (size_t)P.n * (P.kmax + wmax);
         for (int tt = 0; tt * kTR < P.m; ++tt) items_rows.push_back(make_int2(i, tt));
         for (int tt = 0; tt * kTR < P.n; ++tt) items_cols.push_back(make_int2(i, tt));
       }
@@ -1236,6 +1306,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       oa.st = dst.p;
       oa.ws = ws.p;
       oa.bs = bs;
+      oa.bst = 0;
       oa.thresh2 = thresh2;
       // FP32 working precision and d <= 3: specialised tensor-core sketch
       // kernels; otherwise the SIMT kernel in the working precision
@@ -1243,10 +1314,11 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       const bool fast = kTensor && t->d <= 3;
       KmmFastArgs kf{};
       DevBuf<uint2> om2;
-      int bs0 = bs_first;  // first round's sample width
+      // round 0 basis columns: as wide as every block's rank cap allows
+      int bs0 = bs_first;
       for (const Prob& P : bp)
-        if (P.kmax < bs0) bs0 = bs;
-      const int bs8 = (bs0 + 7) & ~7;
+        if (P.kmax < bs0) bs0 = std::max(bs, P.kmax / 8 * 8);
+      const int bs8 = (bs0 + bst + 7) & ~7;
       int om_rows2 = 0;
       if (fast) {
         int max_n = 1;
@@ -1278,13 +1350,14 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       const int max_rounds = kMaxCols / bs + 2;
       for (int round = 0; round < max_rounds; ++round) {
         if (fast) {
-          const int rbs = round == 0 ? bs0 : bs;
+          const int rbs = (round == 0 ? bs0 : bs) + bst;  // basis + test columns
           k_omega_pack<<<592, 256, 0, stream>>>(om2.p, om_rows2 / 8, rbs, bs8 / 8, ka.seed, round);
           HM_LAUNCH_CHECK();
           kf.round = round;
           kf.bs = rbs;
           kf.items = drows.p;
           oa.bs = rbs;
+          oa.bst = bst;
           launch_kmm_fast(t->d, opt.kernel, 0, (rbs + 7) / 8, (unsigned)items_rows.size(), stream, kf);
         } else {
           ka.mode = 0;
