@@ -14,6 +14,7 @@
 //   double pts[N*d]; int32 perm[N]; int32 offsets[2^depth+1]
 //   for level in [0, depth): double bmin[2^level*d], bmax[2^level*d]
 //   int32 numTiles[numLevels]; for l in [0, numLevels-1): int32 tiles[numTiles[l]]
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -64,11 +65,16 @@ int main(int argc, char** argv) {
     CK(cudaMemcpy(h_pts.data(), d_pts, sizeof(double) * N * d, cudaMemcpyDeviceToHost));
   }
 
+  // wall time of the reference's own stages (device synchronised), printed
+  // with the summary line for baseline measurements
+  auto now = [] { return std::chrono::steady_clock::now(); };
+  auto t0 = now();
   KDTree tree;
   allocateKDTree(tree, N, d, b, FULL_TREE);
   constructKDTree(N, d, b, tree, d_pts, FULL_TREE);
   CK(cudaGetLastError());
   CK(cudaDeviceSynchronize());
+  auto t1 = now();
 
   int depth = getMaxSegmentSize((int)N, (int)b).second;
   int nleaf = 1 << depth;
@@ -77,10 +83,13 @@ int main(int argc, char** argv) {
   CK(cudaMemcpy(offs.data(), tree.segmentOffsets, sizeof(int) * (nleaf + 1),
                 cudaMemcpyDeviceToHost));
 
+  auto t2 = now();
   HMatrixStructure st;
   constructHMatrixStructure(&st, upperPowerOfTwo((int)N), d, b,
                             admiss ? BOX_CENTER_ADMISSIBILITY : WEAK_ADMISSIBILITY,
                             tree.boundingBoxes, tree.boundingBoxes);
+  CK(cudaDeviceSynchronize());
+  auto t3 = now();
 
   FILE* f = fopen(out, "wb");
   if (!f) return 1;
@@ -98,8 +107,9 @@ int main(int argc, char** argv) {
   fwrite(st.numTiles, sizeof(int), st.numLevels, f);
   for (int l = 0; l < st.numLevels - 1; ++l) fwrite(st.tileIndices[l], sizeof(int), st.numTiles[l], f);
   fclose(f);
-  printf("ref_pipeline: N=%u d=%u b=%u admiss=%d depth=%d levels=%d\n", N, d, b, admiss, depth,
-         st.numLevels);
+  printf("ref_pipeline: N=%u d=%u b=%u admiss=%d depth=%d levels=%d kdtree_ms=%.3f structure_ms=%.3f\n", N,
+         d, b, admiss, depth, st.numLevels, std::chrono::duration<double, std::milli>(t1 - t0).count(),
+         std::chrono::duration<double, std::milli>(t3 - t2).count());
   freeKDTree(tree);
   cudaFree(d_pts);
   return 0;
