@@ -249,6 +249,11 @@ HM_API hm_status hm_hmatrix_blocks(hm_hmatrix h, long long* num_lowrank, long lo
  * column-major, A_block ~ U V^T. */
 HM_API hm_status hm_hmatrix_block_factors(hm_hmatrix h, int i, float* U, float* V);
 
+/* Host copy of stored dense block i (m x n, column-major, FP32; the order of
+ * hm_hmatrix_blocks' dense rows).  Diagonal blocks recomputed from the
+ * coordinates (diag_from_coords) are not stored and not listed. */
+HM_API hm_status hm_hmatrix_dense_block(hm_hmatrix h, int i, float* D);
+
 HM_API void hm_hmatrix_free(hm_hmatrix h);
 
 /* Schedule autotuner (no counterpart in the reference).  Times the product's

@@ -1739,6 +1739,14 @@ hm_status hm_hmatrix_block_factors(hm_hmatrix h, int i, float* U, float* V) {
   return HM_OK;
 }
 
+hm_status hm_hmatrix_dense_block(hm_hmatrix h, int i, float* D) {
+  if (!h) return hm::fail(HM_ERR_INVALID, "hm_hmatrix_dense_block: null matrix");
+  if (i < 0 || (size_t)i >= h->h_dense.size()) return hm::fail(HM_ERR_INVALID, "hm_hmatrix_dense_block: bad index");
+  const hm::DenseBlock& b = h->h_dense[i];
+  if (D && b.m && b.n) HM_CUDA(cudaMemcpy(D, b.D, sizeof(float) * (size_t)b.m * b.n, cudaMemcpyDeviceToHost));
+  return HM_OK;
+}
+
 void hm_hmatrix_free(hm_hmatrix h) { delete h; }
 
 }  // extern "C"
