@@ -1,18 +1,23 @@
 // hm_mixed.cu -- mixed-precision H-matvec: BF16 hi + lo factor panels on the
 // tensor cores (mma.sync m16n8k16, FP32 accumulation).
 //
-// One product of <= 16 right-hand sides runs four or five kernels:
+// One product of <= 16 right-hand sides runs three or four kernels:
 //   k_mx_split_x  X (FP32, tree order) -> BF16 hi + lo fragments per 32-row tile
 //   k_mx_p1       P = panel^T X per (panel, column group, row chunk); a panel
-//                 projected in one row chunk stores P, indexed by its global
-//                 column tile, else each chunk's partial
+//                 projected in one row chunk stores P as T, else each chunk's
+//                 partial
 //   k_mx_reduce   (panels of several row chunks only) the partials summed in
-//                 chunk order into P
-//   k_mx_gather   T = P with every column moved to the column of the panel
-//                 that expands it (the mirror block's factor), split hi + lo
+//                 chunk order, stored as T
 //   k_mx_p2       Y = sum over the ancestors' panels of U T, plus dense blocks
-// All stores are whole 16-byte fragment words; only the gather reads single
-// floats (the permutation moves whole block runs, so its reads stay local).
+// "Stored as T": the projection on a factor column is the coefficient of the
+// mirror block's factor column (block (s,t) = U V^T: V^T X_t multiplies U,
+// U^T X_s multiplies V), so each column of P is written, split into BF16
+// hi + lo, to the column that it multiplies.  T keeps each column's hi and lo
+// in one 32-bit word per right-hand side, so that any column lands on its own
+// (8 bytes per lane: right-hand sides g and g + 8) and no permutation pass is
+// needed.  Phase 2 reads that word as a k-pair of the B operand and feeds the
+// factor column twice (both halves of the A pair hold U[r][c]), so that one
+// MMA gives U (T_hi + T_lo) over 8 columns.
 // Each product of a BF16 pair uses three MMAs (hi*lo, lo*hi, hi*hi; lo*lo is
 // below FP32 rounding); the low-part MMA of a factor is skipped for the tiles
 // that carry none.  The tensor core's internal sums do not round to nearest, so
@@ -31,6 +36,56 @@ namespace {
 
 __device__ __forceinline__ void mma_a4(float (&d)[4], const uint4& a, uint32_t b0, uint32_t b1) {
   mma_bf16(d, a.x, a.y, a.z, a.w, b0, b1);
+}
+
+// An L2 policy that keeps lines over streamed ones: the X fragments are read
+// once per tree level by phase 1 (and again by phase 2's dense blocks), while
+// the panels stream past them with evict-first loads.
+__device__ __forceinline__ uint64_t l2_keep_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint4 ld_keep(const uint4* ptr, uint64_t pol) {
+  uint4 v;
+  asm volatile("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;\n"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(ptr), "l"(pol));
+  return v;
+}
+
+// T layout: tile (8 columns) x lane (g,t) x {column 2t at right-hand sides g
+// and g + 8, column 2t + 1 at g and g + 8}, each entry bf16x2 {hi, lo}: the
+// two B-operand k-pairs of lane (g,t) for both 8-wide right-hand-side tiles.
+__device__ __forceinline__ long long t_slot(long long col, int g) {  // uint2 index of (column, lane row g)
+  return (((col >> 3) * 32 + 4 * g + ((col & 7) >> 1)) << 1) + (col & 1);
+}
+
+// One lane's C fragment of projection tile `col_tile` (global column tile:
+// columns 2t and 2t+1 at right-hand sides g and g + 8), stored as T: each
+// column to its mirror's slot, split hi + lo; a padding column (no mirror)
+// writes zeros to its own slot, which is the padding of the same panel in T,
+// so that every T word is written once per product.
+__device__ __forceinline__ void mx_store_t(uint4* __restrict__ T, const int* __restrict__ mirror,
+                                           long long col_tile, int lane, float a0, float a1, float a2, float a3) {
+  const int g = lane >> 2;
+  const long long c0 = col_tile * 8 + 2 * (lane & 3);
+  int2 m;  // loaded here, after the projection's loop (a volatile load is not hoisted into it)
+  asm volatile("ld.global.nc.v2.s32 {%0, %1}, [%2];\n" : "=r"(m.x), "=r"(m.y) : "l"(mirror + c0));
+  uint32_t h, l, h8, l8;
+  split_bf16x2(a0, a1, h, l);    // right-hand side g:     columns 2t, 2t+1
+  split_bf16x2(a2, a3, h8, l8);  // right-hand side g + 8
+  const uint2 z = make_uint2(0u, 0u);
+  const uint2 w0 = m.x >= 0 ? make_uint2(__byte_perm(h, l, 0x5410), __byte_perm(h8, l8, 0x5410)) : z;
+  const uint2 w1 = m.y >= 0 ? make_uint2(__byte_perm(h, l, 0x7632), __byte_perm(h8, l8, 0x7632)) : z;
+  const long long d0 = m.x >= 0 ? m.x : c0, d1 = m.y >= 0 ? m.y : c0 + 1;
+  uint2* T2 = reinterpret_cast<uint2*>(T);
+  if (d1 == d0 + 1 && (d0 & 1) == 0) {  // a whole word of the destination tile
+    reinterpret_cast<uint4*>(T2 + t_slot(d0, g))[0] = make_uint4(w0.x, w0.y, w1.x, w1.y);
+  } else {
+    T2[t_slot(d0, g)] = w0;
+    T2[t_slot(d1, g)] = w1;
+  }
 }
 
 // ---- X -> fragments ---------------------------------------------------------
@@ -70,12 +125,13 @@ __global__ void __launch_bounds__(128) k_mx_split_x(const float* __restrict__ X,
 // row tiles.  NCT: column tiles compiled for, RU: row tiles loaded per step.
 template <int NCT, int RU>
 __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, const uint4* __restrict__ store,
-                                           const uint4* __restrict__ Xf, float4* __restrict__ S,
-                                           float4* __restrict__ Pr, int lane) {
+                                           const uint4* __restrict__ Xf, const int* __restrict__ mirror,
+                                           float4* __restrict__ S, uint4* __restrict__ T, int lane) {
   float acc[NCT][4];
 #pragma unroll
   for (int j = 0; j < NCT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
   const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+  const uint64_t keep = l2_keep_policy();
   for (int r = 0; r < u.nrt; r += RU) {
     uint4 xf[RU][4], vh[RU][NCT], vl[RU][NCT];
 #pragma unroll
@@ -84,7 +140,7 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
       const long long rt = u.rt0 + r + q;
       const uint4* xp = Xf + (size_t)(P.tile0 + rt) * 128 + lane;
 #pragma unroll
-      for (int p = 0; p < 4; ++p) xf[q][p] = ok ? __ldg(xp + p * 32) : z;
+      for (int p = 0; p < 4; ++p) xf[q][p] = ok ? ld_keep(xp + p * 32, keep) : z;
       const uint4* hp = store + (P.hi1 + rt * P.nct + u.ct0) * 32 + lane;
       const uint4* lp = store + (P.lo1 + rt * P.nctl + u.ct0) * 32 + lane;
 #pragma unroll
@@ -114,31 +170,36 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
       }
     }
   }
-  // the whole projection (indexed by global column tile) or one chunk's partial
-  float4* out = P.nchunk == 1 ? Pr + (P.t0 + u.ct0) * 32 + lane
-                              : S + (P.s0 + (long long)u.chunk * P.nct + u.ct0) * 32 + lane;
+  // the whole projection, stored as T, or one chunk's partial
+  if (P.nchunk == 1) {
 #pragma unroll
-  for (int j = 0; j < NCT; ++j)
-    if (j < u.nct) out[j * 32] = make_float4(acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+    for (int j = 0; j < NCT; ++j)
+      if (j < u.nct) mx_store_t(T, mirror, P.t0 + u.ct0 + j, lane, acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+  } else {
+    float4* out = S + (P.s0 + (long long)u.chunk * P.nct + u.ct0) * 32 + lane;
+#pragma unroll
+    for (int j = 0; j < NCT; ++j)
+      if (j < u.nct) out[j * 32] = make_float4(acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+  }
 }
 
 // (four CTAs per SM: more warps keep more loads in flight; measured faster
 // than three despite a few spilled registers)
 __global__ void __launch_bounds__(128, 4) k_mx_p1(const MxUnit* __restrict__ units, int nunits,
                                                const MxPanel* __restrict__ panels, const uint4* __restrict__ store,
-                                               const uint4* __restrict__ Xf, float4* __restrict__ S,
-                                               float4* __restrict__ Pr) {
+                                               const uint4* __restrict__ Xf, const int* __restrict__ mirror,
+                                               float4* __restrict__ S, uint4* __restrict__ T) {
   const int w = blockIdx.x * 4 + (threadIdx.x >> 5);
   if (w >= nunits) return;
   const int lane = threadIdx.x & 31;
   const MxUnit u = units[w];
   const MxPanel P = panels[u.panel];
   if (u.nct > 4)
-    mx_p1_unit<8, 1>(u, P, store, Xf, S, Pr, lane);
+    mx_p1_unit<8, 1>(u, P, store, Xf, mirror, S, T, lane);
   else if (u.nct > 2)
-    mx_p1_unit<4, 2>(u, P, store, Xf, S, Pr, lane);
+    mx_p1_unit<4, 2>(u, P, store, Xf, mirror, S, T, lane);
   else
-    mx_p1_unit<2, 4>(u, P, store, Xf, S, Pr, lane);
+    mx_p1_unit<2, 4>(u, P, store, Xf, mirror, S, T, lane);
 }
 
 // ---- phase 1, persistent warps with a cp.async ring --------------------------
@@ -168,8 +229,8 @@ template <int WARPS, int RING, int VT>
 __global__ void __launch_bounds__(32 * WARPS, 1) k_mx_p1r(const MxUnit* __restrict__ units, int nunits,
                                                           const MxPanel* __restrict__ panels,
                                                           const uint4* __restrict__ store,
-                                                          const uint4* __restrict__ Xf, float4* __restrict__ S,
-                                                          float4* __restrict__ Pr) {
+                                                          const uint4* __restrict__ Xf, const int* __restrict__ mirror,
+                                                          float4* __restrict__ S, uint4* __restrict__ T) {
   constexpr int SLOTS = 4 + 2 * VT;
   extern __shared__ __align__(16) uint4 ring[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -256,11 +317,15 @@ __global__ void __launch_bounds__(32 * WARPS, 1) k_mx_p1r(const MxUnit* __restri
         add4(acc[j], d[j]);
       }
     if (++crt == CU.nrt) {
-      float4* out = CP.nchunk == 1 ? Pr + (CP.t0 + CU.ct0) * 32 + lane
-                                   : S + (CP.s0 + (long long)CU.chunk * CP.nct + CU.ct0) * 32 + lane;
+      float4* out = S + (CP.s0 + (long long)CU.chunk * CP.nct + CU.ct0) * 32 + lane;
 #pragma unroll
       for (int j = 0; j < VT; ++j) {
-        if (j < CU.nct) out[j * 32] = make_float4(acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+        if (j < CU.nct) {
+          if (CP.nchunk == 1)
+            mx_store_t(T, mirror, CP.t0 + CU.ct0 + j, lane, acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+          else
+            out[j * 32] = make_float4(acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+        }
         acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
       }
       crt = 0;
@@ -277,9 +342,9 @@ __global__ void __launch_bounds__(32 * WARPS, 1) k_mx_p1r(const MxUnit* __restri
 
 // ---- row-chunk reduction ------------------------------------------------------
 // For panels projected in several row chunks: the chunk partials of each
-// column tile summed in chunk order (deterministic) into P.
+// column tile summed in chunk order (deterministic), stored as T.
 __global__ void k_mx_reduce(const int2* __restrict__ mtiles, long long nmt, const MxPanel* __restrict__ panels,
-                            const float4* __restrict__ S, float4* __restrict__ Pr) {
+                            const float4* __restrict__ S, const int* __restrict__ mirror, uint4* __restrict__ T) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nmt * 32) return;
   const int2 mt = mtiles[i >> 5];  // (panel, column tile)
@@ -293,36 +358,7 @@ __global__ void k_mx_reduce(const int2* __restrict__ mtiles, long long nmt, cons
     v.z += a.z;
     v.w += a.w;
   }
-  Pr[(P.t0 + mt.y) * 32 + lane] = v;
-}
-
-// ---- column gather ----------------------------------------------------------
-// T tile word of lane (g,t) = {hi(T[2t][g], T[2t+1][g]), hi(.. g+8), lo(.. g), lo(.. g+8)}
-// with T[c][r] = P[tinv[c]][r] (0 for padding).  P tile (C fragment): lane
-// (g,t) = {P[2t][g], P[2t+1][g], P[2t][g+8], P[2t+1][g+8]}.
-__global__ void k_mx_gather(const int* __restrict__ tinv, long long t_tiles, const float* __restrict__ Pr,
-                            uint4* __restrict__ T) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= t_tiles * 32) return;
-  const long long tile = i >> 5;
-  const int lane = (int)(i & 31), g = lane >> 2, t = lane & 3;
-  float v[2][2];
-#pragma unroll
-  for (int c = 0; c < 2; ++c) {
-    const int sc = __ldg(tinv + tile * 8 + 2 * t + c);
-    float a = 0.f, b = 0.f;
-    if (sc >= 0) {
-      const float* p = Pr + (size_t)(sc >> 3) * 128 + (4 * g + ((sc & 7) >> 1)) * 4 + (sc & 1);
-      a = __ldg(p);
-      b = __ldg(p + 2);
-    }
-    v[c][0] = a;
-    v[c][1] = b;
-  }
-  uint4 o;
-  split_bf16x2(v[0][0], v[1][0], o.x, o.z);
-  split_bf16x2(v[0][1], v[1][1], o.y, o.w);
-  T[i] = o;
+  mx_store_t(T, mirror, P.t0 + mt.y, lane, v.x, v.y, v.z, v.w);
 }
 
 // ---- phase 2 ----------------------------------------------------------------
@@ -342,6 +378,39 @@ __device__ __forceinline__ void mx_p2_step(float (&acc)[2][2][4], const uint4& h
       mma_bf16(d, a0, a1, a2, a3, bh[nb][0], bh[nb][1]);
       add4(acc[mt][nb], d);
     }
+  }
+}
+
+// acc[mt][nb] += U (32 rows x 8 columns, one tile h) (T_hi + T_lo) (8 x 16):
+// the factor's column pair {c, c+1} of each row becomes two k-pairs
+// {U[r][c], U[r][c]} and {U[r][c+1], U[r][c+1]}, against the T words {hi, lo}
+// of columns c and c+1, so that one MMA sums U (T_hi + T_lo) over 8 columns.
+__device__ __forceinline__ void mx_p2_tile(float (&d)[2][2][4], const uint4& h, const uint4& tw) {
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt) {
+    const uint32_t r0 = mt ? h.z : h.x, r8 = mt ? h.w : h.y;  // rows g (+16), g + 8 (+16)
+    const uint32_t a0 = __byte_perm(r0, 0u, 0x1010), a1 = __byte_perm(r8, 0u, 0x1010);
+    const uint32_t a2 = __byte_perm(r0, 0u, 0x3232), a3 = __byte_perm(r8, 0u, 0x3232);
+    mma_bf16(d[mt][0], a0, a1, a2, a3, tw.x, tw.z);  // right-hand sides 0-7
+    mma_bf16(d[mt][1], a0, a1, a2, a3, tw.y, tw.w);  // right-hand sides 8-15
+  }
+}
+
+// acc += U_lo T_hi for two tiles ct, ct + 1 in one MMA per output tile: the
+// k-pairs are {column c of tile ct, column c of tile ct + 1}, the B halves the
+// hi parts of the two tiles' T words.  (U_lo T_lo is below FP32 rounding.)
+__device__ __forceinline__ void mx_p2_lo_pair(float (&d)[2][2][4], const uint4& l0, const uint4& l1,
+                                              const uint4& t0, const uint4& t1) {
+  const uint32_t b00 = __byte_perm(t0.x, t1.x, 0x5410), b01 = __byte_perm(t0.z, t1.z, 0x5410);
+  const uint32_t b10 = __byte_perm(t0.y, t1.y, 0x5410), b11 = __byte_perm(t0.w, t1.w, 0x5410);
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt) {
+    const uint32_t r0 = mt ? l0.z : l0.x, s0 = mt ? l1.z : l1.x;
+    const uint32_t r8 = mt ? l0.w : l0.y, s8 = mt ? l1.w : l1.y;
+    const uint32_t a0 = __byte_perm(r0, s0, 0x5410), a1 = __byte_perm(r8, s8, 0x5410);
+    const uint32_t a2 = __byte_perm(r0, s0, 0x7632), a3 = __byte_perm(r8, s8, 0x7632);
+    mma_bf16(d[mt][0], a0, a1, a2, a3, b00, b01);
+    mma_bf16(d[mt][1], a0, a1, a2, a3, b10, b11);
   }
 }
 
@@ -403,9 +472,19 @@ __global__ void __launch_bounds__(128, 7) k_mx_p2(int num_tiles, int depth, cons
       const uint4 l1 = lo1 ? __ldcs(ul + (ct + 1) * 32) : z;
       const uint4 t0 = __ldg(tt + ct * 32);
       const uint4 t1 = two ? __ldg(tt + (ct + 1) * 32) : z;
-      const uint32_t bh[2][2] = {{t0.x, t1.x}, {t0.y, t1.y}};
-      const uint32_t bl[2][2] = {{t0.z, t1.z}, {t0.w, t1.w}};
-      mx_p2_step(acc, h0, h1, l0, l1, bh, bl, lo0);
+      // one chain per two tiles, low parts first (a zero tile adds exact zeros)
+      float d[2][2][4];
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nb = 0; nb < 2; ++nb) d[mt][nb][0] = d[mt][nb][1] = d[mt][nb][2] = d[mt][nb][3] = 0.f;
+      if (lo0) mx_p2_lo_pair(d, l0, l1, t0, t1);
+      mx_p2_tile(d, h0, t0);
+      if (two) mx_p2_tile(d, h1, t1);
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nb = 0; nb < 2; ++nb) add4(acc[mt][nb], d[mt][nb]);
     }
   }
   for (int q = leaf_dptr[x]; q < leaf_dptr[x + 1]; ++q) {
@@ -641,8 +720,9 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   }
 
   // column sources and the projection's column map
+  if ((long long)t_tiles * 8 > 0x7fffffffll) return fail(HM_ERR_UNSUPPORTED, "mixed form: too many factor columns");
   std::vector<const float*> colsrc((size_t)t_tiles * 8, nullptr);
-  std::vector<int> tinv((size_t)t_tiles * 8, -1);  // partner column (an involution)
+  std::vector<int> mirror((size_t)t_tiles * 8, -1);  // partner column (an involution)
   long long bytes_lr = 0;
   for (size_t i = 0; i < pairs.size(); ++i) {
     const MxPair& q = pairs[i];
@@ -654,8 +734,8 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
       const int cv = c < q.khi ? colL_v[i] + c : colH_v[i] + c - q.khi;
       colsrc[bu + cu] = q.fu + (size_t)c * q.m;
       colsrc[bv + cv] = q.fv + (size_t)c * q.n;
-      tinv[bv + cv] = (int)(bu + cu);  // Y_u += fu (fv^T X_v)
-      tinv[bu + cu] = (int)(bv + cv);  // Y_v += fv (fu^T X_u)
+      mirror[bv + cv] = (int)(bu + cu);  // Y_u += fu (fv^T X_v)
+      mirror[bu + cu] = (int)(bv + cv);  // Y_v += fv (fu^T X_u)
     }
     bytes_lr += 2ll * (q.m + q.n) * (q.k + q.khi);
   }
@@ -703,8 +783,7 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   HM_TRY(upload(M.pan_of, pan_of, s));
   HM_TRY(upload(M.tile_leaf, tile_leaf, s));
   HM_TRY(upload(M.leaf_tile0, leaf_tile0, s));
-  if ((long long)t_tiles * 8 > 0x7fffffffll) return fail(HM_ERR_UNSUPPORTED, "mixed form: too many factor columns");
-  HM_TRY(upload(M.tinv, tinv, s));
+  HM_TRY(upload(M.mirror, mirror, s));
   HM_TRY(upload(M.dense, dense, s));
   HM_TRY(upload(M.leaf_dptr, dptr, s));
   HM_TRY(upload(M.leaf_dblk, dblk, s));
@@ -806,8 +885,7 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
   MxPlan& M = h->mx;
   uint4* Xf = reinterpret_cast<uint4*>(scratch);
   float4* S = reinterpret_cast<float4*>(scratch + (size_t)M.num_tiles * 4 * 128);
-  float4* Pr = S + (size_t)M.s_tiles * 32;
-  uint4* T = reinterpret_cast<uint4*>(Pr + (size_t)M.t_tiles * 32);
+  uint4* T = reinterpret_cast<uint4*>(S + (size_t)M.s_tiles * 32);
   const int* leaf_off = h->tree->offsets.p;
   if (M.num_tiles > 0) {
     k_mx_split_x<<<(M.num_tiles + 3) / 4, 128, 0, s>>>(X, ldx, nr, M.num_tiles, M.tile_leaf.p, M.leaf_tile0.p,
@@ -818,26 +896,22 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
   if (M.num_units > 0) {
     if (M.p1_ring && M.group_tiles <= 4) {
       k_mx_p1r<8, 3, 4><<<M.num_sms, 256, ring_smem<8, 3, 4>(), s>>>(M.units.p, M.num_units, M.panels.p, M.store.p,
-                                                                      Xf, S, Pr);
+                                                                      Xf, M.mirror.p, S, T);
     } else if (M.p1_ring) {
       k_mx_p1r<4, 4, 8><<<M.num_sms, 128, ring_smem<4, 4, 8>(), s>>>(M.units.p, M.num_units, M.panels.p, M.store.p,
-                                                                      Xf, S, Pr);
+                                                                      Xf, M.mirror.p, S, T);
     } else {
-      k_mx_p1<<<(M.num_units + 3) / 4, 128, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf, S, Pr);
+      k_mx_p1<<<(M.num_units + 3) / 4, 128, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf,
+                                                    M.mirror.p, S, T);
     }
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_mx_p1", M.bytes_p1 + 4ll * h->n * 16, s);
   }
   if (M.nmt > 0) {
-    k_mx_reduce<<<(unsigned)((M.nmt * 32 + 255) / 256), 256, 0, s>>>(M.mtiles.p, M.nmt, M.panels.p, S, Pr);
+    k_mx_reduce<<<(unsigned)((M.nmt * 32 + 255) / 256), 256, 0, s>>>(M.mtiles.p, M.nmt, M.panels.p, S,
+                                                                      M.mirror.p, T);
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_mx_reduce", 512ll * M.s_tiles + 512ll * M.nmt, s);
-  }
-  if (M.t_tiles > 0) {
-    k_mx_gather<<<(unsigned)((M.t_tiles * 32 + 255) / 256), 256, 0, s>>>(M.tinv.p, M.t_tiles,
-                                                                         reinterpret_cast<const float*>(Pr), T);
-    HM_LAUNCH_CHECK();
-    if (km) km->mark("k_mx_gather", 2ll * h->stats.rank_sum * 16 * 4, s);
   }
   if (M.num_tiles > 0) {
     k_mx_p2<<<(M.num_tiles + 3) / 4, 128, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,

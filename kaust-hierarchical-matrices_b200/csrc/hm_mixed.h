@@ -65,7 +65,8 @@ struct MxPlan {
   DevBuf<int> tile_leaf;   // global row tile -> leaf
   DevBuf<int> leaf_tile0;  // leaf -> first global row tile (num_leaves + 1)
   int num_tiles = 0;
-  DevBuf<int> tinv;        // global factor column (8 * t0 + c) -> its mirror column, or -1 (padding)
+  DevBuf<int> mirror;      // global factor column (8 * t0 + c) -> its mirror column, or -1 (padding);
+                           // an involution on the factor columns
   DevBuf<int2> mtiles;     // (panel, column tile) of panels projected in several row chunks
   long long nmt = 0;
   long long s_tiles = 0, t_tiles = 0;
@@ -78,9 +79,9 @@ struct MxPlan {
   bool p1_ring = false;                    // phase 1 by persistent warps with a cp.async ring
   int num_sms = 148;
   // scratch of one 16-column panel of right-hand sides, in floats: X
-  // fragments, chunk partials, projections P (by source column), T (by
-  // expanding column, BF16 hi + lo)
-  long long scratch_floats() const { return ((long long)num_tiles * 4 + s_tiles + 2 * t_tiles) * 128; }
+  // fragments, chunk partials, T (the projections by expanding column, BF16
+  // hi + lo)
+  long long scratch_floats() const { return ((long long)num_tiles * 4 + s_tiles + t_tiles) * 128; }
 };
 
 struct MxPair {  // one stored low-rank pair (u rows, v columns) = fu fv^T, and its mirror
