@@ -15,9 +15,8 @@
 // hi + lo, to the column that it multiplies.  T keeps each column's hi and lo
 // in one 32-bit word per right-hand side, so that any column lands on its own
 // (8 bytes per lane: right-hand sides g and g + 8) and no permutation pass is
-// needed.  Phase 2 reads that word as a k-pair of the B operand and feeds the
-// factor column twice (both halves of the A pair hold U[r][c]), so that one
-// MMA gives U (T_hi + T_lo) over 8 columns.
+// needed.  Phase 2 rebuilds its B operand pairs {T[c], T[c+1]} (hi, and lo)
+// from two such words with one byte permute each.
 // Each product of a BF16 pair uses three MMAs (hi*lo, lo*hi, hi*hi; lo*lo is
 // below FP32 rounding); the low-part MMA of a factor is skipped for the tiles
 // that carry none.  The tensor core's internal sums do not round to nearest, so
@@ -57,35 +56,35 @@ __device__ __forceinline__ uint4 ld_keep(const uint4* ptr, uint64_t pol) {
 // T layout: tile (8 columns) x lane (g,t) x {column 2t at right-hand sides g
 // and g + 8, column 2t + 1 at g and g + 8}, each entry bf16x2 {hi, lo}: the
 // two B-operand k-pairs of lane (g,t) for both 8-wide right-hand-side tiles.
-__device__ __forceinline__ long long t_slot(long long col, int g) {  // uint2 index of (column, lane row g)
+__host__ __device__ __forceinline__ long long t_slot(long long col, int g) {  // uint2 index of (column, row g)
   return (((col >> 3) * 32 + 4 * g + ((col & 7) >> 1)) << 1) + (col & 1);
 }
 
-// One lane's C fragment of projection tile `col_tile` (global column tile:
-// columns 2t and 2t+1 at right-hand sides g and g + 8), stored as T: each
-// column to its mirror's slot, split hi + lo; a padding column (no mirror)
-// writes zeros to its own slot, which is the padding of the same panel in T,
-// so that every T word is written once per product.
-__device__ __forceinline__ void mx_store_t(uint4* __restrict__ T, const int* __restrict__ mirror,
-                                           long long col_tile, int lane, float a0, float a1, float a2, float a3) {
+// One lane's C fragment of a projection tile (columns 2t and 2t+1 at
+// right-hand sides g and g + 8), stored as T: each column to its mirror's slot
+// (m: the tslot entries of columns 2t, 2t+1), split hi + lo; a padding column
+// (no mirror) writes zeros to its own slot, which is the padding of the same
+// panel in T, so that every T word is written once per product.
+__device__ __forceinline__ void mx_store_t(uint4* __restrict__ T, int2 m, int lane, float a0, float a1, float a2,
+                                           float a3) {
   const int g = lane >> 2;
-  const long long c0 = col_tile * 8 + 2 * (lane & 3);
-  int2 m;  // loaded here, after the projection's loop (a volatile load is not hoisted into it)
-  asm volatile("ld.global.nc.v2.s32 {%0, %1}, [%2];\n" : "=r"(m.x), "=r"(m.y) : "l"(mirror + c0));
   uint32_t h, l, h8, l8;
   split_bf16x2(a0, a1, h, l);    // right-hand side g:     columns 2t, 2t+1
   split_bf16x2(a2, a3, h8, l8);  // right-hand side g + 8
   const uint2 z = make_uint2(0u, 0u);
   const uint2 w0 = m.x >= 0 ? make_uint2(__byte_perm(h, l, 0x5410), __byte_perm(h8, l8, 0x5410)) : z;
   const uint2 w1 = m.y >= 0 ? make_uint2(__byte_perm(h, l, 0x7632), __byte_perm(h8, l8, 0x7632)) : z;
-  const long long d0 = m.x >= 0 ? m.x : c0, d1 = m.y >= 0 ? m.y : c0 + 1;
+  const int s0 = (m.x >= 0 ? m.x : -1 - m.x) + 8 * g, s1 = (m.y >= 0 ? m.y : -1 - m.y) + 8 * g;
   uint2* T2 = reinterpret_cast<uint2*>(T);
-  if (d1 == d0 + 1 && (d0 & 1) == 0) {  // a whole word of the destination tile
-    reinterpret_cast<uint4*>(T2 + t_slot(d0, g))[0] = make_uint4(w0.x, w0.y, w1.x, w1.y);
+  if (s1 == s0 + 1 && (s0 & 1) == 0) {  // a whole word of the destination tile
+    *reinterpret_cast<uint4*>(T2 + s0) = make_uint4(w0.x, w0.y, w1.x, w1.y);
   } else {
-    T2[t_slot(d0, g)] = w0;
-    T2[t_slot(d1, g)] = w1;
+    T2[s0] = w0;
+    T2[s1] = w1;
   }
+}
+__device__ __forceinline__ int2 tslot_pair(const int* __restrict__ tslot, long long col_tile, int lane) {
+  return __ldg(reinterpret_cast<const int2*>(tslot + col_tile * 8 + 2 * (lane & 3)));
 }
 
 // ---- X -> fragments ---------------------------------------------------------
@@ -125,13 +124,17 @@ __global__ void __launch_bounds__(128) k_mx_split_x(const float* __restrict__ X,
 // row tiles.  NCT: column tiles compiled for, RU: row tiles loaded per step.
 template <int NCT, int RU>
 __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, const uint4* __restrict__ store,
-                                           const uint4* __restrict__ Xf, const int* __restrict__ mirror,
+                                           const uint4* __restrict__ Xf, const int* __restrict__ tslot,
                                            float4* __restrict__ S, uint4* __restrict__ T, int lane) {
   float acc[NCT][4];
 #pragma unroll
   for (int j = 0; j < NCT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
   const uint4 z = make_uint4(0u, 0u, 0u, 0u);
   const uint64_t keep = l2_keep_policy();
+  // the mirrors of the unit's columns, fetched now so that the stores after
+  // the loop wait for nothing: lane 4j + t holds tile j's pair t
+  int2 mm = make_int2(-1, -1);
+  if (P.nchunk == 1 && lane < 4 * NCT && (lane >> 2) < u.nct) mm = tslot_pair(tslot, P.t0 + u.ct0 + (lane >> 2), lane);
   for (int r = 0; r < u.nrt; r += RU) {
     uint4 xf[RU][4], vh[RU][NCT], vl[RU][NCT];
 #pragma unroll
@@ -174,7 +177,11 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
   if (P.nchunk == 1) {
 #pragma unroll
     for (int j = 0; j < NCT; ++j)
-      if (j < u.nct) mx_store_t(T, mirror, P.t0 + u.ct0 + j, lane, acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+      if (j < u.nct) {
+        const int src = 4 * j + (lane & 3);
+        const int2 m = make_int2(__shfl_sync(0xffffffffu, mm.x, src), __shfl_sync(0xffffffffu, mm.y, src));
+        mx_store_t(T, m, lane, acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+      }
   } else {
     float4* out = S + (P.s0 + (long long)u.chunk * P.nct + u.ct0) * 32 + lane;
 #pragma unroll
@@ -187,7 +194,7 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
 // than three despite a few spilled registers)
 __global__ void __launch_bounds__(128, 4) k_mx_p1(const MxUnit* __restrict__ units, int nunits,
                                                const MxPanel* __restrict__ panels, const uint4* __restrict__ store,
-                                               const uint4* __restrict__ Xf, const int* __restrict__ mirror,
+                                               const uint4* __restrict__ Xf, const int* __restrict__ tslot,
                                                float4* __restrict__ S, uint4* __restrict__ T) {
   const int w = blockIdx.x * 4 + (threadIdx.x >> 5);
   if (w >= nunits) return;
@@ -195,11 +202,11 @@ __global__ void __launch_bounds__(128, 4) k_mx_p1(const MxUnit* __restrict__ uni
   const MxUnit u = units[w];
   const MxPanel P = panels[u.panel];
   if (u.nct > 4)
-    mx_p1_unit<8, 1>(u, P, store, Xf, mirror, S, T, lane);
+    mx_p1_unit<8, 1>(u, P, store, Xf, tslot, S, T, lane);
   else if (u.nct > 2)
-    mx_p1_unit<4, 2>(u, P, store, Xf, mirror, S, T, lane);
+    mx_p1_unit<4, 2>(u, P, store, Xf, tslot, S, T, lane);
   else
-    mx_p1_unit<2, 4>(u, P, store, Xf, mirror, S, T, lane);
+    mx_p1_unit<2, 4>(u, P, store, Xf, tslot, S, T, lane);
 }
 
 // ---- phase 1, persistent warps with a cp.async ring --------------------------
@@ -229,7 +236,7 @@ template <int WARPS, int RING, int VT>
 __global__ void __launch_bounds__(32 * WARPS, 1) k_mx_p1r(const MxUnit* __restrict__ units, int nunits,
                                                           const MxPanel* __restrict__ panels,
                                                           const uint4* __restrict__ store,
-                                                          const uint4* __restrict__ Xf, const int* __restrict__ mirror,
+                                                          const uint4* __restrict__ Xf, const int* __restrict__ tslot,
                                                           float4* __restrict__ S, uint4* __restrict__ T) {
   constexpr int SLOTS = 4 + 2 * VT;
   extern __shared__ __align__(16) uint4 ring[];
@@ -322,7 +329,8 @@ __global__ void __launch_bounds__(32 * WARPS, 1) k_mx_p1r(const MxUnit* __restri
       for (int j = 0; j < VT; ++j) {
         if (j < CU.nct) {
           if (CP.nchunk == 1)
-            mx_store_t(T, mirror, CP.t0 + CU.ct0 + j, lane, acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+            mx_store_t(T, tslot_pair(tslot, CP.t0 + CU.ct0 + j, lane), lane, acc[j][0], acc[j][1], acc[j][2],
+                       acc[j][3]);
           else
             out[j * 32] = make_float4(acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
         }
@@ -344,7 +352,7 @@ __global__ void __launch_bounds__(32 * WARPS, 1) k_mx_p1r(const MxUnit* __restri
 // For panels projected in several row chunks: the chunk partials of each
 // column tile summed in chunk order (deterministic), stored as T.
 __global__ void k_mx_reduce(const int2* __restrict__ mtiles, long long nmt, const MxPanel* __restrict__ panels,
-                            const float4* __restrict__ S, const int* __restrict__ mirror, uint4* __restrict__ T) {
+                            const float4* __restrict__ S, const int* __restrict__ tslot, uint4* __restrict__ T) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nmt * 32) return;
   const int2 mt = mtiles[i >> 5];  // (panel, column tile)
@@ -358,7 +366,7 @@ __global__ void k_mx_reduce(const int2* __restrict__ mtiles, long long nmt, cons
     v.z += a.z;
     v.w += a.w;
   }
-  mx_store_t(T, mirror, P.t0 + mt.y, lane, v.x, v.y, v.z, v.w);
+  mx_store_t(T, tslot_pair(tslot, P.t0 + mt.y, lane), lane, v.x, v.y, v.z, v.w);
 }
 
 // ---- phase 2 ----------------------------------------------------------------
@@ -378,39 +386,6 @@ __device__ __forceinline__ void mx_p2_step(float (&acc)[2][2][4], const uint4& h
       mma_bf16(d, a0, a1, a2, a3, bh[nb][0], bh[nb][1]);
       add4(acc[mt][nb], d);
     }
-  }
-}
-
-// acc[mt][nb] += U (32 rows x 8 columns, one tile h) (T_hi + T_lo) (8 x 16):
-// the factor's column pair {c, c+1} of each row becomes two k-pairs
-// {U[r][c], U[r][c]} and {U[r][c+1], U[r][c+1]}, against the T words {hi, lo}
-// of columns c and c+1, so that one MMA sums U (T_hi + T_lo) over 8 columns.
-__device__ __forceinline__ void mx_p2_tile(float (&d)[2][2][4], const uint4& h, const uint4& tw) {
-#pragma unroll
-  for (int mt = 0; mt < 2; ++mt) {
-    const uint32_t r0 = mt ? h.z : h.x, r8 = mt ? h.w : h.y;  // rows g (+16), g + 8 (+16)
-    const uint32_t a0 = __byte_perm(r0, 0u, 0x1010), a1 = __byte_perm(r8, 0u, 0x1010);
-    const uint32_t a2 = __byte_perm(r0, 0u, 0x3232), a3 = __byte_perm(r8, 0u, 0x3232);
-    mma_bf16(d[mt][0], a0, a1, a2, a3, tw.x, tw.z);  // right-hand sides 0-7
-    mma_bf16(d[mt][1], a0, a1, a2, a3, tw.y, tw.w);  // right-hand sides 8-15
-  }
-}
-
-// acc += U_lo T_hi for two tiles ct, ct + 1 in one MMA per output tile: the
-// k-pairs are {column c of tile ct, column c of tile ct + 1}, the B halves the
-// hi parts of the two tiles' T words.  (U_lo T_lo is below FP32 rounding.)
-__device__ __forceinline__ void mx_p2_lo_pair(float (&d)[2][2][4], const uint4& l0, const uint4& l1,
-                                              const uint4& t0, const uint4& t1) {
-  const uint32_t b00 = __byte_perm(t0.x, t1.x, 0x5410), b01 = __byte_perm(t0.z, t1.z, 0x5410);
-  const uint32_t b10 = __byte_perm(t0.y, t1.y, 0x5410), b11 = __byte_perm(t0.w, t1.w, 0x5410);
-#pragma unroll
-  for (int mt = 0; mt < 2; ++mt) {
-    const uint32_t r0 = mt ? l0.z : l0.x, s0 = mt ? l1.z : l1.x;
-    const uint32_t r8 = mt ? l0.w : l0.y, s8 = mt ? l1.w : l1.y;
-    const uint32_t a0 = __byte_perm(r0, s0, 0x5410), a1 = __byte_perm(r8, s8, 0x5410);
-    const uint32_t a2 = __byte_perm(r0, s0, 0x7632), a3 = __byte_perm(r8, s8, 0x7632);
-    mma_bf16(d[mt][0], a0, a1, a2, a3, b00, b01);
-    mma_bf16(d[mt][1], a0, a1, a2, a3, b10, b11);
   }
 }
 
@@ -472,19 +447,12 @@ __global__ void __launch_bounds__(128, 7) k_mx_p2(int num_tiles, int depth, cons
       const uint4 l1 = lo1 ? __ldcs(ul + (ct + 1) * 32) : z;
       const uint4 t0 = __ldg(tt + ct * 32);
       const uint4 t1 = two ? __ldg(tt + (ct + 1) * 32) : z;
-      // one chain per two tiles, low parts first (a zero tile adds exact zeros)
-      float d[2][2][4];
-#pragma unroll
-      for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int nb = 0; nb < 2; ++nb) d[mt][nb][0] = d[mt][nb][1] = d[mt][nb][2] = d[mt][nb][3] = 0.f;
-      if (lo0) mx_p2_lo_pair(d, l0, l1, t0, t1);
-      mx_p2_tile(d, h0, t0);
-      if (two) mx_p2_tile(d, h1, t1);
-#pragma unroll
-      for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int nb = 0; nb < 2; ++nb) add4(acc[mt][nb], d[mt][nb]);
+      // B pairs {T[2t], T[2t+1]} per tile from the per-column {hi, lo} words
+      const uint32_t bh[2][2] = {{__byte_perm(t0.x, t0.z, 0x5410), __byte_perm(t1.x, t1.z, 0x5410)},
+                                 {__byte_perm(t0.y, t0.w, 0x5410), __byte_perm(t1.y, t1.w, 0x5410)}};
+      const uint32_t bl[2][2] = {{__byte_perm(t0.x, t0.z, 0x7632), __byte_perm(t1.x, t1.z, 0x7632)},
+                                 {__byte_perm(t0.y, t0.w, 0x7632), __byte_perm(t1.y, t1.w, 0x7632)}};
+      mx_p2_step(acc, h0, h1, l0, l1, bh, bl, lo0);
     }
   }
   for (int q = leaf_dptr[x]; q < leaf_dptr[x + 1]; ++q) {
@@ -720,7 +688,7 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   }
 
   // column sources and the projection's column map
-  if ((long long)t_tiles * 8 > 0x7fffffffll) return fail(HM_ERR_UNSUPPORTED, "mixed form: too many factor columns");
+  if ((long long)t_tiles * 64 > 0x7fffffffll) return fail(HM_ERR_UNSUPPORTED, "mixed form: too many factor columns");
   std::vector<const float*> colsrc((size_t)t_tiles * 8, nullptr);
   std::vector<int> mirror((size_t)t_tiles * 8, -1);  // partner column (an involution)
   long long bytes_lr = 0;
@@ -783,7 +751,10 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   HM_TRY(upload(M.pan_of, pan_of, s));
   HM_TRY(upload(M.tile_leaf, tile_leaf, s));
   HM_TRY(upload(M.leaf_tile0, leaf_tile0, s));
-  HM_TRY(upload(M.mirror, mirror, s));
+  std::vector<int> tslot(mirror.size());
+  for (size_t c = 0; c < mirror.size(); ++c)
+    tslot[c] = mirror[c] >= 0 ? (int)t_slot(mirror[c], 0) : -1 - (int)t_slot((long long)c, 0);
+  HM_TRY(upload(M.tslot, tslot, s));
   HM_TRY(upload(M.dense, dense, s));
   HM_TRY(upload(M.leaf_dptr, dptr, s));
   HM_TRY(upload(M.leaf_dblk, dblk, s));
@@ -896,20 +867,20 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
   if (M.num_units > 0) {
     if (M.p1_ring && M.group_tiles <= 4) {
       k_mx_p1r<8, 3, 4><<<M.num_sms, 256, ring_smem<8, 3, 4>(), s>>>(M.units.p, M.num_units, M.panels.p, M.store.p,
-                                                                      Xf, M.mirror.p, S, T);
+                                                                      Xf, M.tslot.p, S, T);
     } else if (M.p1_ring) {
       k_mx_p1r<4, 4, 8><<<M.num_sms, 128, ring_smem<4, 4, 8>(), s>>>(M.units.p, M.num_units, M.panels.p, M.store.p,
-                                                                      Xf, M.mirror.p, S, T);
+                                                                      Xf, M.tslot.p, S, T);
     } else {
       k_mx_p1<<<(M.num_units + 3) / 4, 128, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf,
-                                                    M.mirror.p, S, T);
+                                                    M.tslot.p, S, T);
     }
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_mx_p1", M.bytes_p1 + 4ll * h->n * 16, s);
   }
   if (M.nmt > 0) {
     k_mx_reduce<<<(unsigned)((M.nmt * 32 + 255) / 256), 256, 0, s>>>(M.mtiles.p, M.nmt, M.panels.p, S,
-                                                                      M.mirror.p, T);
+                                                                      M.tslot.p, T);
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_mx_reduce", 512ll * M.s_tiles + 512ll * M.nmt, s);
   }

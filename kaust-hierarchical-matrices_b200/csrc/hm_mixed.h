@@ -65,8 +65,11 @@ struct MxPlan {
   DevBuf<int> tile_leaf;   // global row tile -> leaf
   DevBuf<int> leaf_tile0;  // leaf -> first global row tile (num_leaves + 1)
   int num_tiles = 0;
-  DevBuf<int> mirror;      // global factor column (8 * t0 + c) -> its mirror column, or -1 (padding);
-                           // an involution on the factor columns
+  // global factor column (8 * t0 + c) -> the 8-byte slot of T (lane row 0;
+  // row g adds 8 g) that its projection fills: its mirror column's slot (the
+  // mirror map is an involution on the factor columns), or -1 - its own slot
+  // for a padding column, which fills that slot with zeros
+  DevBuf<int> tslot;
   DevBuf<int2> mtiles;     // (panel, column tile) of panels projected in several row chunks
   long long nmt = 0;
   long long s_tiles = 0, t_tiles = 0;
