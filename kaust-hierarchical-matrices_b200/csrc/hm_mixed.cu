@@ -190,13 +190,15 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
   }
 }
 
-// (four CTAs per SM: more warps keep more loads in flight; measured faster
-// than three despite a few spilled registers)
-__global__ void __launch_bounds__(128, 4) k_mx_p1(const MxUnit* __restrict__ units, int nunits,
+// One warp per CTA, 16 per SM (measured): a warp runs one unit and retires at
+// once, instead of holding its CTA's slot until three sibling warps with
+// other units finish; 16 warps keep enough loads in flight at 128 registers.
+constexpr int kP1Warps = 1, kP1PerSm = 16;
+__global__ void __launch_bounds__(32 * kP1Warps, kP1PerSm / kP1Warps) k_mx_p1(const MxUnit* __restrict__ units, int nunits,
                                                const MxPanel* __restrict__ panels, const uint4* __restrict__ store,
                                                const uint4* __restrict__ Xf, const int* __restrict__ tslot,
                                                float4* __restrict__ S, uint4* __restrict__ T) {
-  const int w = blockIdx.x * 4 + (threadIdx.x >> 5);
+  const int w = blockIdx.x * kP1Warps + (threadIdx.x >> 5);
   if (w >= nunits) return;
   const int lane = threadIdx.x & 31;
   const MxUnit u = units[w];
@@ -391,15 +393,17 @@ __device__ __forceinline__ void mx_p2_step(float (&acc)[2][2][4], const uint4& h
 
 // One warp per global row tile (32 rows of one leaf): every ancestor cluster's
 // panel rows times its T, then the dense blocks of the leaf row.
-// (seven CTAs per SM: the kernel is bound by loads in flight, not registers)
-__global__ void __launch_bounds__(128, 7) k_mx_p2(int num_tiles, int depth, const int* __restrict__ tile_leaf,
+// (one warp per CTA, 28 per SM, measured: the kernel is bound by loads in
+// flight, and a warp that finishes its row tile frees its slot at once)
+constexpr int kP2Warps = 1, kP2PerSm = 28;  // warps per CTA (one row tile each), warps per SM
+__global__ void __launch_bounds__(32 * kP2Warps, kP2PerSm / kP2Warps) k_mx_p2(int num_tiles, int depth, const int* __restrict__ tile_leaf,
                                                const int* __restrict__ leaf_tile0, const int* __restrict__ leaf_off,
                                                const int* __restrict__ pan_of, const MxPanel* __restrict__ panels,
                                                const uint4* __restrict__ store, const uint4* __restrict__ T,
                                                const int* __restrict__ leaf_dptr, const int* __restrict__ leaf_dblk,
                                                const MxDense* __restrict__ dense, const uint4* __restrict__ Xf,
                                                float* __restrict__ Y, int ldy, int nr) {
-  const int G = blockIdx.x * 4 + (threadIdx.x >> 5);
+  const int G = blockIdx.x * kP2Warps + (threadIdx.x >> 5);
   if (G >= num_tiles) return;
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int x = tile_leaf[G];
@@ -872,7 +876,7 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
       k_mx_p1r<4, 4, 8><<<M.num_sms, 128, ring_smem<4, 4, 8>(), s>>>(M.units.p, M.num_units, M.panels.p, M.store.p,
                                                                       Xf, M.tslot.p, S, T);
     } else {
-      k_mx_p1<<<(M.num_units + 3) / 4, 128, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf,
+      k_mx_p1<<<(M.num_units + kP1Warps - 1) / kP1Warps, 32 * kP1Warps, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf,
                                                     M.tslot.p, S, T);
     }
     HM_LAUNCH_CHECK();
@@ -885,7 +889,7 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
     if (km) km->mark("k_mx_reduce", 512ll * M.s_tiles + 512ll * M.nmt, s);
   }
   if (M.num_tiles > 0) {
-    k_mx_p2<<<(M.num_tiles + 3) / 4, 128, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
+    k_mx_p2<<<(M.num_tiles + kP2Warps - 1) / kP2Warps, 32 * kP2Warps, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
                                                   M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p,
                                                   M.leaf_dblk.p, M.dense.p, Xf, Y, ldy, nr);
     HM_LAUNCH_CHECK();
