@@ -16,7 +16,10 @@
 // in one 32-bit word per right-hand side, so that any column lands on its own
 // (8 bytes per lane: right-hand sides g and g + 8) and no permutation pass is
 // needed.  Phase 2 rebuilds its B operand pairs {T[c], T[c+1]} (hi, and lo)
-// from two such words with one byte permute each.
+// from two such words with one byte permute each.  A factor column without a
+// low part (its block's small singular directions, where the factor's own
+// BF16 rounding is within the budget) gets T's hi only: one word holds
+// right-hand sides g and g + 8, and phase 2 multiplies U_hi T_hi alone.
 // Each product of a BF16 pair uses three MMAs (hi*lo, lo*hi, hi*hi; lo*lo is
 // below FP32 rounding); the low-part MMA of a factor is skipped for the tiles
 // that carry none.  The tensor core's internal sums do not round to nearest, so
@@ -53,34 +56,53 @@ __device__ __forceinline__ uint4 ld_keep(const uint4* ptr, uint64_t pol) {
   return v;
 }
 
-// T layout: tile (8 columns) x lane (g,t) x {column 2t at right-hand sides g
-// and g + 8, column 2t + 1 at g and g + 8}, each entry bf16x2 {hi, lo}: the
-// two B-operand k-pairs of lane (g,t) for both 8-wide right-hand-side tiles.
-__host__ __device__ __forceinline__ long long t_slot(long long col, int g) {  // uint2 index of (column, row g)
-  return (((col >> 3) * 32 + 4 * g + ((col & 7) >> 1)) << 1) + (col & 1);
+// T layout, per panel: its nctl tiles with low parts, then the others.
+//   with low parts (128 words): lane (g,t) x {column 2t at right-hand sides g,
+//     g + 8; column 2t + 1 at g, g + 8}, each word bf16x2 {hi, lo}
+//   without (64 words): lane (g,t) x {column 2t, column 2t + 1}, each word
+//     bf16x2 {hi at g, hi at g + 8}
+// Word of (column c of the panel, lane row 0); row g adds 16 g, resp. 8 g.
+__host__ __device__ __forceinline__ long long t_word(long long tw0, int nctl, int c) {
+  const int tile = c >> 3, t = (c & 7) >> 1, odd = c & 1;
+  return tile < nctl ? tw0 + (long long)tile * 128 + 4 * t + 2 * odd
+                     : tw0 + (long long)nctl * 128 + (long long)(tile - nctl) * 64 + 2 * t + odd;
 }
 
 // One lane's C fragment of a projection tile (columns 2t and 2t+1 at
-// right-hand sides g and g + 8), stored as T: each column to its mirror's slot
-// (m: the tslot entries of columns 2t, 2t+1), split hi + lo; a padding column
-// (no mirror) writes zeros to its own slot, which is the padding of the same
-// panel in T, so that every T word is written once per product.
-__device__ __forceinline__ void mx_store_t(uint4* __restrict__ T, int2 m, int lane, float a0, float a1, float a2,
+// right-hand sides g and g + 8), stored as T: each column to its mirror's
+// words (m: the tslot entries of columns 2t, 2t+1), split hi + lo or hi only;
+// a padding column (no mirror) writes zeros to its own words, which are the
+// padding of the same panel in T, so that every T word is written once per
+// product.  Both columns of a pair are of the same kind (a panel's tiles with
+// low parts come first), so the branch is uniform over the warp.
+__device__ __forceinline__ void mx_store_t(uint32_t* __restrict__ T, int2 m, int lane, float a0, float a1, float a2,
                                            float a3) {
   const int g = lane >> 2;
-  uint32_t h, l, h8, l8;
-  split_bf16x2(a0, a1, h, l);    // right-hand side g:     columns 2t, 2t+1
-  split_bf16x2(a2, a3, h8, l8);  // right-hand side g + 8
-  const uint2 z = make_uint2(0u, 0u);
-  const uint2 w0 = m.x >= 0 ? make_uint2(__byte_perm(h, l, 0x5410), __byte_perm(h8, l8, 0x5410)) : z;
-  const uint2 w1 = m.y >= 0 ? make_uint2(__byte_perm(h, l, 0x7632), __byte_perm(h8, l8, 0x7632)) : z;
-  const int s0 = (m.x >= 0 ? m.x : -1 - m.x) + 8 * g, s1 = (m.y >= 0 ? m.y : -1 - m.y) + 8 * g;
-  uint2* T2 = reinterpret_cast<uint2*>(T);
-  if (s1 == s0 + 1 && (s0 & 1) == 0) {  // a whole word of the destination tile
-    *reinterpret_cast<uint4*>(T2 + s0) = make_uint4(w0.x, w0.y, w1.x, w1.y);
-  } else {
-    T2[s0] = w0;
-    T2[s1] = w1;
+  const int e0 = m.x >= 0 ? m.x : -1 - m.x, e1 = m.y >= 0 ? m.y : -1 - m.y;
+  const int o0 = e0 >> 1, o1 = e1 >> 1;
+  if ((e0 & 1) == 0) {  // with low parts: 8 bytes per column
+    uint32_t h, l, h8, l8;
+    split_bf16x2(a0, a1, h, l);    // right-hand side g:     columns 2t, 2t+1
+    split_bf16x2(a2, a3, h8, l8);  // right-hand side g + 8
+    const uint2 z = make_uint2(0u, 0u);
+    const uint2 w0 = m.x >= 0 ? make_uint2(__byte_perm(h, l, 0x5410), __byte_perm(h8, l8, 0x5410)) : z;
+    const uint2 w1 = m.y >= 0 ? make_uint2(__byte_perm(h, l, 0x7632), __byte_perm(h8, l8, 0x7632)) : z;
+    const int s0 = o0 + 16 * g, s1 = o1 + 16 * g;
+    if (s1 == s0 + 2 && (s0 & 3) == 0) {  // a whole 16-byte word of the destination tile
+      *reinterpret_cast<uint4*>(T + s0) = make_uint4(w0.x, w0.y, w1.x, w1.y);
+    } else {
+      *reinterpret_cast<uint2*>(T + s0) = w0;
+      *reinterpret_cast<uint2*>(T + s1) = w1;
+    }
+  } else {  // hi only: 4 bytes per column
+    const uint32_t w0 = m.x >= 0 ? pack_bf16(a0, a2) : 0u, w1 = m.y >= 0 ? pack_bf16(a1, a3) : 0u;
+    const int s0 = o0 + 8 * g, s1 = o1 + 8 * g;
+    if (s1 == s0 + 1 && (s0 & 1) == 0) {
+      *reinterpret_cast<uint2*>(T + s0) = make_uint2(w0, w1);
+    } else {
+      T[s0] = w0;
+      T[s1] = w1;
+    }
   }
 }
 __device__ __forceinline__ int2 tslot_pair(const int* __restrict__ tslot, long long col_tile, int lane) {
@@ -125,7 +147,7 @@ __global__ void __launch_bounds__(128) k_mx_split_x(const float* __restrict__ X,
 template <int NCT, int RU>
 __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, const uint4* __restrict__ store,
                                            const uint4* __restrict__ Xf, const int* __restrict__ tslot,
-                                           float4* __restrict__ S, uint4* __restrict__ T, int lane) {
+                                           float4* __restrict__ S, uint32_t* __restrict__ T, int lane) {
   float acc[NCT][4];
 #pragma unroll
   for (int j = 0; j < NCT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
@@ -197,7 +219,7 @@ constexpr int kP1Warps = 1, kP1PerSm = 16;
 __global__ void __launch_bounds__(32 * kP1Warps, kP1PerSm / kP1Warps) k_mx_p1(const MxUnit* __restrict__ units, int nunits,
                                                const MxPanel* __restrict__ panels, const uint4* __restrict__ store,
                                                const uint4* __restrict__ Xf, const int* __restrict__ tslot,
-                                               float4* __restrict__ S, uint4* __restrict__ T) {
+                                               float4* __restrict__ S, uint32_t* __restrict__ T) {
   const int w = blockIdx.x * kP1Warps + (threadIdx.x >> 5);
   if (w >= nunits) return;
   const int lane = threadIdx.x & 31;
@@ -239,7 +261,7 @@ __global__ void __launch_bounds__(32 * WARPS, 1) k_mx_p1r(const MxUnit* __restri
                                                           const MxPanel* __restrict__ panels,
                                                           const uint4* __restrict__ store,
                                                           const uint4* __restrict__ Xf, const int* __restrict__ tslot,
-                                                          float4* __restrict__ S, uint4* __restrict__ T) {
+                                                          float4* __restrict__ S, uint32_t* __restrict__ T) {
   constexpr int SLOTS = 4 + 2 * VT;
   extern __shared__ __align__(16) uint4 ring[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -354,7 +376,7 @@ __global__ void __launch_bounds__(32 * WARPS, 1) k_mx_p1r(const MxUnit* __restri
 // For panels projected in several row chunks: the chunk partials of each
 // column tile summed in chunk order (deterministic), stored as T.
 __global__ void k_mx_reduce(const int2* __restrict__ mtiles, long long nmt, const MxPanel* __restrict__ panels,
-                            const float4* __restrict__ S, const int* __restrict__ tslot, uint4* __restrict__ T) {
+                            const float4* __restrict__ S, const int* __restrict__ tslot, uint32_t* __restrict__ T) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nmt * 32) return;
   const int2 mt = mtiles[i >> 5];  // (panel, column tile)
@@ -391,6 +413,21 @@ __device__ __forceinline__ void mx_p2_step(float (&acc)[2][2][4], const uint4& h
   }
 }
 
+// acc[mt][nb] += A_hi (16 rows x 16 columns, tiles h0|h1) B_hi (16 x 8)
+__device__ __forceinline__ void mx_p2_step_hi(float (&acc)[2][2][4], const uint4& h0, const uint4& h1,
+                                              const uint32_t (&bh)[2][2]) {
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt) {
+    const uint32_t a0 = mt ? h0.z : h0.x, a1 = mt ? h0.w : h0.y, a2 = mt ? h1.z : h1.x, a3 = mt ? h1.w : h1.y;
+#pragma unroll
+    for (int nb = 0; nb < 2; ++nb) {
+      float d[4] = {0.f, 0.f, 0.f, 0.f};
+      mma_bf16(d, a0, a1, a2, a3, bh[nb][0], bh[nb][1]);
+      add4(acc[mt][nb], d);
+    }
+  }
+}
+
 // One warp per global row tile (32 rows of one leaf): every ancestor cluster's
 // panel rows times its T, then the dense blocks of the leaf row.
 // (one warp per CTA, 28 per SM, measured: the kernel is bound by loads in
@@ -399,7 +436,7 @@ constexpr int kP2Warps = 1, kP2PerSm = 28;  // warps per CTA (one row tile each)
 __global__ void __launch_bounds__(32 * kP2Warps, kP2PerSm / kP2Warps) k_mx_p2(int num_tiles, int depth, const int* __restrict__ tile_leaf,
                                                const int* __restrict__ leaf_tile0, const int* __restrict__ leaf_off,
                                                const int* __restrict__ pan_of, const MxPanel* __restrict__ panels,
-                                               const uint4* __restrict__ store, const uint4* __restrict__ T,
+                                               const uint4* __restrict__ store, const uint32_t* __restrict__ T,
                                                const int* __restrict__ leaf_dptr, const int* __restrict__ leaf_dblk,
                                                const MxDense* __restrict__ dense, const uint4* __restrict__ Xf,
                                                float* __restrict__ Y, int ldy, int nr) {
@@ -426,7 +463,7 @@ __global__ void __launch_bounds__(32 * kP2Warps, kP2PerSm / kP2Warps) k_mx_p2(in
       const long long rt = G - P.tile0;
       my_u = P.hi2 + rt * P.nct;
       my_l = P.lo2 + rt * P.nctl;
-      my_t = P.t0;
+      my_t = P.tw0;
       my_nct = P.nct;
       my_nctl = P.nctl;
     }
@@ -441,22 +478,36 @@ __global__ void __launch_bounds__(32 * kP2Warps, kP2PerSm / kP2Warps) k_mx_p2(in
     const int nctl = __shfl_sync(0xffffffffu, my_nctl, l - 1);
     const uint4* uh = store + ou * 32 + lane;
     const uint4* ul = store + ol * 32 + lane;
-    const uint4* tt = T + ot * 32 + lane;
+    // tiles with low parts: U (hi + lo) T (hi + lo)
+    const uint4* tl = reinterpret_cast<const uint4*>(T + ot) + lane;
 #pragma unroll 2
-    for (int ct = 0; ct < nct; ct += 2) {
-      const bool two = ct + 1 < nct, lo0 = ct < nctl, lo1 = ct + 1 < nctl;
+    for (int ct = 0; ct < nctl; ct += 2) {
+      const bool two = ct + 1 < nctl;
       const uint4 h0 = __ldcs(uh + ct * 32);
       const uint4 h1 = two ? __ldcs(uh + (ct + 1) * 32) : z;
-      const uint4 l0 = lo0 ? __ldcs(ul + ct * 32) : z;
-      const uint4 l1 = lo1 ? __ldcs(ul + (ct + 1) * 32) : z;
-      const uint4 t0 = __ldg(tt + ct * 32);
-      const uint4 t1 = two ? __ldg(tt + (ct + 1) * 32) : z;
+      const uint4 l0 = __ldcs(ul + ct * 32);
+      const uint4 l1 = two ? __ldcs(ul + (ct + 1) * 32) : z;
+      const uint4 t0 = __ldg(tl + ct * 32);
+      const uint4 t1 = two ? __ldg(tl + (ct + 1) * 32) : z;
       // B pairs {T[2t], T[2t+1]} per tile from the per-column {hi, lo} words
       const uint32_t bh[2][2] = {{__byte_perm(t0.x, t0.z, 0x5410), __byte_perm(t1.x, t1.z, 0x5410)},
                                  {__byte_perm(t0.y, t0.w, 0x5410), __byte_perm(t1.y, t1.w, 0x5410)}};
       const uint32_t bl[2][2] = {{__byte_perm(t0.x, t0.z, 0x7632), __byte_perm(t1.x, t1.z, 0x7632)},
                                  {__byte_perm(t0.y, t0.w, 0x7632), __byte_perm(t1.y, t1.w, 0x7632)}};
-      mx_p2_step(acc, h0, h1, l0, l1, bh, bl, lo0);
+      mx_p2_step(acc, h0, h1, l0, l1, bh, bl, true);
+    }
+    // tiles without: U_hi T_hi
+    const uint2* th = reinterpret_cast<const uint2*>(T + ot + (long long)nctl * 128) + lane;
+#pragma unroll 2
+    for (int ct = nctl; ct < nct; ct += 2) {
+      const bool two = ct + 1 < nct;
+      const uint4 h0 = __ldcs(uh + ct * 32);
+      const uint4 h1 = two ? __ldcs(uh + (ct + 1) * 32) : z;
+      const uint2 w0 = __ldg(th + (ct - nctl) * 32);
+      const uint2 w1 = two ? __ldg(th + (ct - nctl + 1) * 32) : make_uint2(0u, 0u);
+      const uint32_t bh[2][2] = {{__byte_perm(w0.x, w0.y, 0x5410), __byte_perm(w1.x, w1.y, 0x5410)},
+                                 {__byte_perm(w0.x, w0.y, 0x7632), __byte_perm(w1.x, w1.y, 0x7632)}};
+      mx_p2_step_hi(acc, h0, h1, bh);
     }
   }
   for (int q = leaf_dptr[x]; q < leaf_dptr[x + 1]; ++q) {
@@ -655,7 +706,7 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   const int np = (int)members.size();
   std::vector<MxPanel> panels(np);
   std::vector<int> colL_u(pairs.size()), colH_u(pairs.size()), colL_v(pairs.size()), colH_v(pairs.size());
-  long long tiles = 0, t_tiles = 0;
+  long long tiles = 0, t_tiles = 0, t_words = 0;
   for (int p = 0; p < np; ++p) {
     long long sl = 0, sh_ = 0;
     for (const Side& m : members[p]) {
@@ -689,10 +740,13 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
     tiles += (long long)P.nrt * P.nctl;
     P.t0 = t_tiles;
     t_tiles += P.nct;
+    P.tw0 = t_words;
+    t_words += (long long)P.nctl * 128 + (long long)(P.nct - P.nctl) * 64;
   }
 
   // column sources and the projection's column map
-  if ((long long)t_tiles * 64 > 0x7fffffffll) return fail(HM_ERR_UNSUPPORTED, "mixed form: too many factor columns");
+  if ((long long)t_tiles * 8 > 0x7fffffffll || t_words >= (1ll << 30))
+    return fail(HM_ERR_UNSUPPORTED, "mixed form: too many factor columns");
   std::vector<const float*> colsrc((size_t)t_tiles * 8, nullptr);
   std::vector<int> mirror((size_t)t_tiles * 8, -1);  // partner column (an involution)
   long long bytes_lr = 0;
@@ -755,9 +809,11 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   HM_TRY(upload(M.pan_of, pan_of, s));
   HM_TRY(upload(M.tile_leaf, tile_leaf, s));
   HM_TRY(upload(M.leaf_tile0, leaf_tile0, s));
-  std::vector<int> tslot(mirror.size());
-  for (size_t c = 0; c < mirror.size(); ++c)
-    tslot[c] = mirror[c] >= 0 ? (int)t_slot(mirror[c], 0) : -1 - (int)t_slot((long long)c, 0);
+  std::vector<int> own(mirror.size()), tslot(mirror.size());  // (word << 1) | no-low-part
+  for (const MxPanel& P : panels)
+    for (int c = 0; c < P.nct * 8; ++c)
+      own[P.t0 * 8 + c] = (int)(t_word(P.tw0, P.nctl, c) << 1) | ((c >> 3) >= P.nctl ? 1 : 0);
+  for (size_t c = 0; c < mirror.size(); ++c) tslot[c] = mirror[c] >= 0 ? own[mirror[c]] : -1 - own[c];
   HM_TRY(upload(M.tslot, tslot, s));
   HM_TRY(upload(M.dense, dense, s));
   HM_TRY(upload(M.leaf_dptr, dptr, s));
@@ -765,6 +821,7 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   M.num_panels = np;
   M.num_dense = (int)dense.size();
   M.t_tiles = t_tiles;
+  M.t_words = t_words;
   // each factor is read once per phase (as V of one orientation in phase 1,
   // as U of the other in phase 2)
   M.bytes_p1 = bytes_lr;
@@ -860,7 +917,7 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
   MxPlan& M = h->mx;
   uint4* Xf = reinterpret_cast<uint4*>(scratch);
   float4* S = reinterpret_cast<float4*>(scratch + (size_t)M.num_tiles * 4 * 128);
-  uint4* T = reinterpret_cast<uint4*>(S + (size_t)M.s_tiles * 32);
+  uint32_t* T = reinterpret_cast<uint32_t*>(S + (size_t)M.s_tiles * 32);
   const int* leaf_off = h->tree->offsets.p;
   if (M.num_tiles > 0) {
     k_mx_split_x<<<(M.num_tiles + 3) / 4, 128, 0, s>>>(X, ldx, nr, M.num_tiles, M.tile_leaf.p, M.leaf_tile0.p,

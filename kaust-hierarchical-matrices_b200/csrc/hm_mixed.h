@@ -34,7 +34,8 @@ namespace hm {
 struct MxPanel {
   long long hi1, lo1, hi2, lo2;  // 512-byte tile offsets into MxPlan::store, [row tile][col tile]
   long long s0;                  // first phase-1 output tile (nchunk x nct tiles)
-  long long t0;                  // first phase-2 input tile (nct tiles)
+  long long t0;                  // first global factor column tile (nct tiles)
+  long long tw0;                 // first 32-bit word of the panel's T (nctl tiles of 128 words, then 64 each)
   int nct, nctl;                 // 8-column tiles; the first nctl carry low parts
   int tile0, nrt;                // first global row tile, row tiles
   int nchunk;                    // row chunks of the projection
@@ -65,14 +66,16 @@ struct MxPlan {
   DevBuf<int> tile_leaf;   // global row tile -> leaf
   DevBuf<int> leaf_tile0;  // leaf -> first global row tile (num_leaves + 1)
   int num_tiles = 0;
-  // global factor column (8 * t0 + c) -> the 8-byte slot of T (lane row 0;
-  // row g adds 8 g) that its projection fills: its mirror column's slot (the
-  // mirror map is an involution on the factor columns), or -1 - its own slot
-  // for a padding column, which fills that slot with zeros
+  // global factor column (8 * t0 + c) -> where its projection goes in T:
+  // (word << 1) | h, word = the column's first 32-bit word at lane row 0 (row
+  // g adds 16 g words in a tile with low parts, 8 g in one without), h = 1
+  // for a tile without low parts.  A data column goes to its mirror column
+  // (the mirror map is an involution on the factor columns); a padding column
+  // is stored as -1 - (its own entry) and fills its own words with zeros.
   DevBuf<int> tslot;
   DevBuf<int2> mtiles;     // (panel, column tile) of panels projected in several row chunks
   long long nmt = 0;
-  long long s_tiles = 0, t_tiles = 0;
+  long long s_tiles = 0, t_tiles = 0, t_words = 0;
   DevBuf<MxDense> dense;
   int num_dense = 0;
   DevBuf<int> leaf_dptr, leaf_dblk;  // dense blocks covering each leaf's rows
@@ -82,9 +85,9 @@ struct MxPlan {
   bool p1_ring = false;                    // phase 1 by persistent warps with a cp.async ring
   int num_sms = 148;
   // scratch of one 16-column panel of right-hand sides, in floats: X
-  // fragments, chunk partials, T (the projections by expanding column, BF16
-  // hi + lo)
-  long long scratch_floats() const { return ((long long)num_tiles * 4 + s_tiles + t_tiles) * 128; }
+  // fragments, chunk partials, T (the projections by expanding column: BF16
+  // hi + lo for the columns with low parts, hi for the others)
+  long long scratch_floats() const { return ((long long)num_tiles * 4 + s_tiles) * 128 + t_words; }
 };
 
 struct MxPair {  // one stored low-rank pair (u rows, v columns) = fu fv^T, and its mirror
