@@ -329,9 +329,11 @@ def run_ours(args):
     clocks = ClockSampler(os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % rank)
                           if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp/bench_clocks_%d.csv" % rank)
     res = {}
-    nr = min(16, nrhs)  # the product runs in panels of 16 right-hand sides
-    panels = (nrhs + 15) // 16
     for f in forms:
+        # the product runs in passes of 32 right-hand sides (mixed form) or 16 (FP32)
+        width = 32 if f == "mixed" else 16
+        nr = min(width, nrhs)
+        panels = (nrhs + width - 1) // width
         ms = timed(step_of(Hs[f]), clocks if f == head else None)
         kt = kernel_times(hm, lib, Hs[f], X, Y, n, nr, stream)
         bp, be = ctypes.c_longlong(), ctypes.c_longlong()
@@ -487,7 +489,7 @@ def run_batch(args):
             _, t = ev_time(lambda: B.build(kernel=kid, ell=w["ell"], nugget=w["nugget"], tol=w["tol"],
                                            max_rank=w["max_rank"], precision=prec, seed=7, stream=s))
             build_s[f] = front_s + t
-            tune[f] = hm.autotune(B.hmatrix(), 16, cache, stream=s)
+            tune[f] = hm.autotune(B.hmatrix(), min(nrhs, 32 if f == "mixed" else 16), cache, stream=s)
             Bs[f] = B
         head = forms[0]
         N = Bs[head].n
@@ -516,13 +518,15 @@ def run_batch(args):
                 clocks.__exit__()
             ms = ranks.max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
             H = B.hmatrix()
-            kt = kernel_times(hm, lib, H, X, Y, N, 16, s)
+            width = 32 if f == "mixed" else 16  # right-hand sides per pass of the product
+            nr = min(width, nrhs)
+            kt = kernel_times(hm, lib, H, X, Y, N, nr, s)
             bp, be = ctypes.c_longlong(), ctypes.c_longlong()
             mp, me = ctypes.c_float(), ctypes.c_float()
-            hm._check(lib.hm_hmatvec_profile(H.h, 16, hm._ptr(X), N, hm._ptr(Y), N, hm._stream(s), ctypes.byref(mp),
+            hm._check(lib.hm_hmatvec_profile(H.h, nr, hm._ptr(X), N, hm._ptr(Y), N, hm._stream(s), ctypes.byref(mp),
                                              ctypes.byref(me), ctypes.byref(bp), ctypes.byref(be)))
-            res[f] = {"ms": ms, "bytes": bp.value + be.value + 12 * N * (nrhs - 16), "kernels": kt,
-                      "panels": (nrhs + 15) // 16, "stats": H.stats()}
+            res[f] = {"ms": ms, "bytes": bp.value + be.value + 12 * N * (nrhs - nr), "kernels": kt,
+                      "panels": (nrhs + width - 1) // width, "stats": H.stats()}
         # e2e: host X in, host Y out, product through hm_batch_matvec
         B = Bs[head]
         Xh = torch.empty((nrhs, N), pin_memory=True)

@@ -218,8 +218,9 @@ HM_API hm_status hm_hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, i
 HM_API hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, int ldx, float* Y, int ldy,
                                     void* stream);
 
-/* hm_hmatvec for one panel (nrhs <= the matrix's panel width, 16 by
- * default), X and Y in tree order, with CUDA events recorded on `stream`
+/* hm_hmatvec for one pass (nrhs <= 16; <= 32 for the mixed form, whose
+ * passes multiply two halves of 16 right-hand sides per factor read), X and Y
+ * in tree order, with CUDA events recorded on `stream`
  * around its two kernels; synchronises and returns each kernel's device time
  * and algorithmic bytes (stored factors and dense blocks read once, X read,
  * Y written).  For measurement; the hot path is hm_hmatvec. */
@@ -227,7 +228,8 @@ HM_API hm_status hm_hmatvec_profile(hm_hmatrix h, int nrhs, const float* X, int 
                                     void* stream, float* ms_project, float* ms_expand,
                                     long long* bytes_project, long long* bytes_expand);
 
-/* Per-kernel device times of one product (nrhs <= 16, X and Y in tree order):
+/* Per-kernel device times of one pass (nrhs as for hm_hmatvec_profile, X and
+ * Y in tree order):
  * CUDA events on `stream` after each kernel, synchronised before return.
  * Fills up to `cap` entries of names (static strings), ms and algorithmic
  * bytes (what the kernel must read and write at least); *count receives the
@@ -257,9 +259,10 @@ HM_API hm_status hm_hmatrix_dense_block(hm_hmatrix h, int i, float* D);
 HM_API void hm_hmatrix_free(hm_hmatrix h);
 
 /* Schedule autotuner (no counterpart in the reference).  Times the product's
- * schedule candidates on this matrix (nrhs columns, <= 16) and keeps the
- * fastest: for the FP32 form the rows of V per phase-1 item, for the mixed
- * form the phase-1 unit shape.  With cache_path set, the choice is appended
+ * schedule candidates on this matrix (nrhs columns, at most one pass of the
+ * product: 16, or 32 for the mixed form) and keeps the fastest: for the FP32
+ * form the rows of V per phase-1 item, for the mixed form the phase-1 unit
+ * shape.  With cache_path set, the choice is appended
  * to that text file under a key of the GPU and the matrix's shape, and a
  * later call whose key is in the file applies the cached choice without
  * timing (*from_cache = 1).  choice receives a description (may be NULL).

@@ -20,6 +20,7 @@
 namespace hm {
 
 hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream);
+int pass_width(hm_hmatrix h);
 
 namespace {
 
@@ -83,7 +84,8 @@ extern "C" hm_status hm_autotune(hm_hmatrix h, int nrhs, const char* cache_path,
                                  char* choice, int choice_len) {
   using namespace hm;
   if (!h) return fail(HM_ERR_INVALID, "hm_autotune: null matrix");
-  if (nrhs < 1 || nrhs > 16) return fail(HM_ERR_INVALID, "hm_autotune: need 1 <= nrhs <= 16");
+  if (nrhs < 1 || nrhs > pass_width(h))
+    return fail(HM_ERR_INVALID, "hm_autotune: need 1 <= nrhs <= one pass of the product (16, or 32 for the mixed form)");
   cudaStream_t s = as_stream(stream);
   const std::string key = shape_key(h, nrhs);
   Choice best;

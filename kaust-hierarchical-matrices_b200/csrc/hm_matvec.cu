@@ -34,6 +34,11 @@
 static __device__ __align__(256) float hm_noalloc_scratch[size_t(4) << 20];
 
 namespace hm {
+
+// Right-hand sides per pass of the product: the mixed form reads every factor
+// tile once for up to two halves of 16, the FP32 form runs 16 at a time.
+int pass_width(hm_hmatrix h) { return h->mx.enabled ? 32 : 16; }
+
 namespace {
 
 constexpr int kWarpsPerCta = 4;
@@ -322,8 +327,9 @@ __global__ void __launch_bounds__(kFlyT) k_diag_fly(const int* __restrict__ leaf
   }
 }
 
-// One panel of nr <= 16 right-hand sides (X, Y in tree order); T: projection
-// scratch (16 x kpad per block, then the chunk partials).
+// One pass of nr <= pass_width(h) right-hand sides (X, Y in tree order); T:
+// projection scratch (FP32 form: 16 x kpad per block, then the chunk
+// partials; mixed form: see mixed_run_panel).
 hm_status run_panel(hm_hmatrix h, int nr, const float* X, int ldx, float* Y, int ldy, float* T, cudaStream_t s,
                     KernelMarks* km) {
   if (h->mx.enabled) return mixed_run_panel(h, nr, X, ldx, Y, ldy, T, s, km);
@@ -454,11 +460,12 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   HM_TRY(P.dense.alloc(std::max<size_t>(h->h_dense.size(), 1)));
   HM_TRY(P.leaf_dptr.alloc(nleaf + 1));
   HM_TRY(P.leaf_dblk.alloc(dblk.size()));
-  // projection scratch of one 16-column panel, for whichever form runs
-  const long long scratch = h->mx.enabled ? h->mx.scratch_floats() : tk + part;
+  // projection scratch of one pass, for whichever form runs (the mixed form
+  // runs passes of up to 32 right-hand sides, the FP32 form 16)
+  const long long scratch = h->mx.enabled ? h->mx.scratch_floats(2) : tk + part;
   HM_TRY(P.T.alloc(std::max<long long>(scratch, 1)));
-  HM_TRY(P.Xp.alloc((size_t)h->n * nrhs_cap));
-  HM_TRY(P.Yp.alloc((size_t)h->n * nrhs_cap));
+  HM_TRY(P.Xp.alloc((size_t)h->n * pass_width(h)));
+  HM_TRY(P.Yp.alloc((size_t)h->n * pass_width(h)));
   auto up = [&](void* dst, const void* src, size_t bytes) -> hm_status {
     if (bytes) HM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
     return HM_OK;
@@ -487,7 +494,7 @@ hm_status hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, int ldx, fl
   MatvecPlan& P = h->plan;
   const int n = h->n;
   for (int c0 = 0; c0 < nrhs;) {
-    const int nr = std::min(16, nrhs - c0);
+    const int nr = std::min(pass_width(h), nrhs - c0);
     const float* Xin = X + (size_t)c0 * ldx;
     float* Yout = Y + (size_t)c0 * ldy;
     const float* Xt = Xin;
@@ -622,8 +629,9 @@ extern "C" hm_status hm_hmatvec_profile(hm_hmatrix h, int nrhs, const float* X, 
                                         void* stream, float* ms_project, float* ms_expand,
                                         long long* bytes_project, long long* bytes_expand) {
   if (!h) return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: null matrix");
-  if (nrhs < 1 || nrhs > 16 || !X || !Y || ldx < h->n || ldy < h->n)
-    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: need 1 <= nrhs <= 16 and valid vectors");
+  if (nrhs < 1 || nrhs > hm::pass_width(h) || !X || !Y || ldx < h->n || ldy < h->n)
+    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: need 1 <= nrhs <= one pass (16, or 32 for the mixed "
+                                    "form) and valid vectors");
   cudaStream_t s = hm::as_stream(stream);
   hm::KernelMarks km;
   HM_TRY(hm::timed_panel(h, nrhs, X, ldx, Y, ldy, s, &km));
@@ -647,8 +655,9 @@ extern "C" hm_status hm_hmatvec_kernels(hm_hmatrix h, int nrhs, const float* X, 
                                         void* stream, int cap, const char** names, float* ms, long long* bytes,
                                         int* count) {
   if (!h) return hm::fail(HM_ERR_INVALID, "hm_hmatvec_kernels: null matrix");
-  if (nrhs < 1 || nrhs > 16 || !X || !Y || ldx < h->n || ldy < h->n || cap < 0)
-    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_kernels: need 1 <= nrhs <= 16 and valid vectors");
+  if (nrhs < 1 || nrhs > hm::pass_width(h) || !X || !Y || ldx < h->n || ldy < h->n || cap < 0)
+    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_kernels: need 1 <= nrhs <= one pass (16, or 32 for the mixed "
+                                    "form) and valid vectors");
   hm::KernelMarks km;
   HM_TRY(hm::timed_panel(h, nrhs, X, ldx, Y, ldy, hm::as_stream(stream), &km));
   for (int i = 0; i < km.n && i < cap; ++i) {

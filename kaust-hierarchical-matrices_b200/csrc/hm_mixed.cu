@@ -121,6 +121,10 @@ __global__ void __launch_bounds__(128) k_mx_split_x(const float* __restrict__ X,
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int G = blockIdx.x * 4 + w;
   if (G >= num_tiles) return;  // whole warp; only warp-level syncs below
+  // half y of a pass of up to 32 right-hand sides: columns 16 y .. 16 y + 15
+  X += (size_t)16 * blockIdx.y * ldx;
+  nr -= 16 * blockIdx.y;
+  Xf += (size_t)blockIdx.y * num_tiles * 128;
   const int x = tile_leaf[G];
   const int row = leaf_off[x] + 32 * (G - leaf_tile0[x]) + lane;
   const bool ok = row < leaf_off[x + 1];
@@ -142,15 +146,21 @@ __global__ void __launch_bounds__(128) k_mx_split_x(const float* __restrict__ X,
 }
 
 // ---- phase 1 ----------------------------------------------------------------
-// C (16 right-hand sides x 8 columns) per column tile = X^T V over the unit's
-// row tiles.  NCT: column tiles compiled for, RU: row tiles loaded per step.
-template <int NCT, int RU>
+// C (16 right-hand sides x 8 columns) per column tile and half = X^T V over
+// the unit's row tiles.  NCT: column tiles compiled for, RU: row tiles loaded
+// per step, NH: halves of 16 right-hand sides (each V tile is loaded once for
+// both); a half's X fragments, S and T sit xh, sh and th elements after the
+// previous half's.
+template <int NCT, int RU, int NH>
 __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, const uint4* __restrict__ store,
                                            const uint4* __restrict__ Xf, const int* __restrict__ tslot,
-                                           float4* __restrict__ S, uint32_t* __restrict__ T, int lane) {
-  float acc[NCT][4];
+                                           float4* __restrict__ S, uint32_t* __restrict__ T, long long xh,
+                                           long long sh, long long th, int lane) {
+  float acc[NH][NCT][4];
 #pragma unroll
-  for (int j = 0; j < NCT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  for (int h = 0; h < NH; ++h)
+#pragma unroll
+    for (int j = 0; j < NCT; ++j) acc[h][j][0] = acc[h][j][1] = acc[h][j][2] = acc[h][j][3] = 0.f;
   const uint4 z = make_uint4(0u, 0u, 0u, 0u);
   const uint64_t keep = l2_keep_policy();
   // the mirrors of the unit's columns, fetched now so that the stores after
@@ -158,14 +168,16 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
   int2 mm = make_int2(-1, -1);
   if (P.nchunk == 1 && lane < 4 * NCT && (lane >> 2) < u.nct) mm = tslot_pair(tslot, P.t0 + u.ct0 + (lane >> 2), lane);
   for (int r = 0; r < u.nrt; r += RU) {
-    uint4 xf[RU][4], vh[RU][NCT], vl[RU][NCT];
+    uint4 xf[RU][NH][4], vh[RU][NCT], vl[RU][NCT];
 #pragma unroll
     for (int q = 0; q < RU; ++q) {
       const bool ok = r + q < u.nrt;
       const long long rt = u.rt0 + r + q;
       const uint4* xp = Xf + (size_t)(P.tile0 + rt) * 128 + lane;
 #pragma unroll
-      for (int p = 0; p < 4; ++p) xf[q][p] = ok ? ld_keep(xp + p * 32, keep) : z;
+      for (int h = 0; h < NH; ++h)
+#pragma unroll
+        for (int p = 0; p < 4; ++p) xf[q][h][p] = ok ? ld_keep(xp + h * xh + p * 32, keep) : z;
       const uint4* hp = store + (P.hi1 + rt * P.nct + u.ct0) * 32 + lane;
       const uint4* lp = store + (P.lo1 + rt * P.nctl + u.ct0) * 32 + lane;
 #pragma unroll
@@ -180,16 +192,19 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
 #pragma unroll
         for (int j = 0; j < NCT; ++j) {
           if (j < u.nct) {
-            float d[4] = {0.f, 0.f, 0.f, 0.f};
-            mma_a4(d, xf[q][2], vh[q][j].x, vh[q][j].y);  // X_lo V_hi
-            mma_a4(d, xf[q][3], vh[q][j].z, vh[q][j].w);
-            if (u.ct0 + j < P.nctl) {                     // X_hi V_lo
-              mma_a4(d, xf[q][0], vl[q][j].x, vl[q][j].y);
-              mma_a4(d, xf[q][1], vl[q][j].z, vl[q][j].w);
+#pragma unroll
+            for (int h = 0; h < NH; ++h) {
+              float d[4] = {0.f, 0.f, 0.f, 0.f};
+              mma_a4(d, xf[q][h][2], vh[q][j].x, vh[q][j].y);  // X_lo V_hi
+              mma_a4(d, xf[q][h][3], vh[q][j].z, vh[q][j].w);
+              if (u.ct0 + j < P.nctl) {                        // X_hi V_lo
+                mma_a4(d, xf[q][h][0], vl[q][j].x, vl[q][j].y);
+                mma_a4(d, xf[q][h][1], vl[q][j].z, vl[q][j].w);
+              }
+              mma_a4(d, xf[q][h][0], vh[q][j].x, vh[q][j].y);  // X_hi V_hi
+              mma_a4(d, xf[q][h][1], vh[q][j].z, vh[q][j].w);
+              add4(acc[h][j], d);
             }
-            mma_a4(d, xf[q][0], vh[q][j].x, vh[q][j].y);  // X_hi V_hi
-            mma_a4(d, xf[q][1], vh[q][j].z, vh[q][j].w);
-            add4(acc[j], d);
           }
         }
       }
@@ -202,13 +217,17 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
       if (j < u.nct) {
         const int src = 4 * j + (lane & 3);
         const int2 m = make_int2(__shfl_sync(0xffffffffu, mm.x, src), __shfl_sync(0xffffffffu, mm.y, src));
-        mx_store_t(T, m, lane, acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+#pragma unroll
+        for (int h = 0; h < NH; ++h)
+          mx_store_t(T + h * th, m, lane, acc[h][j][0], acc[h][j][1], acc[h][j][2], acc[h][j][3]);
       }
   } else {
     float4* out = S + (P.s0 + (long long)u.chunk * P.nct + u.ct0) * 32 + lane;
 #pragma unroll
-    for (int j = 0; j < NCT; ++j)
-      if (j < u.nct) out[j * 32] = make_float4(acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+    for (int h = 0; h < NH; ++h)
+#pragma unroll
+      for (int j = 0; j < NCT; ++j)
+        if (j < u.nct) out[h * sh + j * 32] = make_float4(acc[h][j][0], acc[h][j][1], acc[h][j][2], acc[h][j][3]);
   }
 }
 
@@ -216,21 +235,36 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
 // once, instead of holding its CTA's slot until three sibling warps with
 // other units finish; 16 warps keep enough loads in flight at 128 registers.
 constexpr int kP1Warps = 1, kP1PerSm = 16;
+template <int NH>
 __global__ void __launch_bounds__(32 * kP1Warps, kP1PerSm / kP1Warps) k_mx_p1(const MxUnit* __restrict__ units, int nunits,
                                                const MxPanel* __restrict__ panels, const uint4* __restrict__ store,
                                                const uint4* __restrict__ Xf, const int* __restrict__ tslot,
-                                               float4* __restrict__ S, uint32_t* __restrict__ T) {
+                                               float4* __restrict__ S, uint32_t* __restrict__ T, long long xh,
+                                               long long sh, long long th) {
   const int w = blockIdx.x * kP1Warps + (threadIdx.x >> 5);
   if (w >= nunits) return;
   const int lane = threadIdx.x & 31;
   const MxUnit u = units[w];
   const MxPanel P = panels[u.panel];
-  if (u.nct > 4)
-    mx_p1_unit<8, 1>(u, P, store, Xf, tslot, S, T, lane);
-  else if (u.nct > 2)
-    mx_p1_unit<4, 2>(u, P, store, Xf, tslot, S, T, lane);
-  else
-    mx_p1_unit<2, 4>(u, P, store, Xf, tslot, S, T, lane);
+  if (NH == 1) {
+    if (u.nct > 4)
+      mx_p1_unit<8, 1, 1>(u, P, store, Xf, tslot, S, T, xh, sh, th, lane);
+    else if (u.nct > 2)
+      mx_p1_unit<4, 2, 1>(u, P, store, Xf, tslot, S, T, xh, sh, th, lane);
+    else
+      mx_p1_unit<2, 4, 1>(u, P, store, Xf, tslot, S, T, xh, sh, th, lane);
+  } else if (u.nct > 2) {  // two halves: at most four column tiles at a time
+    MxUnit a = u;
+    a.nct = min(u.nct, 4);
+    mx_p1_unit<4, 1, NH>(a, P, store, Xf, tslot, S, T, xh, sh, th, lane);
+    if (u.nct > 4) {
+      a.ct0 = u.ct0 + 4;
+      a.nct = u.nct - 4;
+      mx_p1_unit<4, 1, NH>(a, P, store, Xf, tslot, S, T, xh, sh, th, lane);
+    }
+  } else {
+    mx_p1_unit<2, 2, NH>(u, P, store, Xf, tslot, S, T, xh, sh, th, lane);
+  }
 }
 
 // ---- phase 1, persistent warps with a cp.async ring --------------------------
@@ -376,9 +410,12 @@ __global__ void __launch_bounds__(32 * WARPS, 1) k_mx_p1r(const MxUnit* __restri
 // For panels projected in several row chunks: the chunk partials of each
 // column tile summed in chunk order (deterministic), stored as T.
 __global__ void k_mx_reduce(const int2* __restrict__ mtiles, long long nmt, const MxPanel* __restrict__ panels,
-                            const float4* __restrict__ S, const int* __restrict__ tslot, uint32_t* __restrict__ T) {
+                            const float4* __restrict__ S, const int* __restrict__ tslot, uint32_t* __restrict__ T,
+                            long long sh, long long th) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nmt * 32) return;
+  S += blockIdx.y * sh;  // half y of the pass
+  T += blockIdx.y * th;
   const int2 mt = mtiles[i >> 5];  // (panel, column tile)
   const int lane = (int)(i & 31);
   const MxPanel P = panels[mt.x];
@@ -432,23 +469,30 @@ __device__ __forceinline__ void mx_p2_step_hi(float (&acc)[2][2][4], const uint4
 // panel rows times its T, then the dense blocks of the leaf row.
 // (one warp per CTA, 28 per SM, measured: the kernel is bound by loads in
 // flight, and a warp that finishes its row tile frees its slot at once)
-constexpr int kP2Warps = 1, kP2PerSm = 28;  // warps per CTA (one row tile each), warps per SM
-__global__ void __launch_bounds__(32 * kP2Warps, kP2PerSm / kP2Warps) k_mx_p2(int num_tiles, int depth, const int* __restrict__ tile_leaf,
+// With two halves of 16 right-hand sides every U tile is loaded once for both,
+// and the warp holds twice the accumulators (16 warps per SM, 128 registers).
+constexpr int kP2Warps = 1, kP2PerSm = 28, kP2PerSm2 = 16;
+template <int NH>
+__global__ void __launch_bounds__(32 * kP2Warps, (NH == 1 ? kP2PerSm : kP2PerSm2) / kP2Warps)
+    k_mx_p2(int num_tiles, int depth, const int* __restrict__ tile_leaf,
                                                const int* __restrict__ leaf_tile0, const int* __restrict__ leaf_off,
                                                const int* __restrict__ pan_of, const MxPanel* __restrict__ panels,
                                                const uint4* __restrict__ store, const uint32_t* __restrict__ T,
                                                const int* __restrict__ leaf_dptr, const int* __restrict__ leaf_dblk,
                                                const MxDense* __restrict__ dense, const uint4* __restrict__ Xf,
-                                               float* __restrict__ Y, int ldy, int nr) {
+                                               float* __restrict__ Y, int ldy, int nr, long long xh_, long long th) {
   const int G = blockIdx.x * kP2Warps + (threadIdx.x >> 5);
   if (G >= num_tiles) return;
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int x = tile_leaf[G];
-  float acc[2][2][4];
+  float acc[NH][2][2][4];
 #pragma unroll
-  for (int mt = 0; mt < 2; ++mt)
+  for (int h = 0; h < NH; ++h)
 #pragma unroll
-    for (int nb = 0; nb < 2; ++nb) acc[mt][nb][0] = acc[mt][nb][1] = acc[mt][nb][2] = acc[mt][nb][3] = 0.f;
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nb = 0; nb < 2; ++nb)
+        acc[h][mt][nb][0] = acc[h][mt][nb][1] = acc[h][mt][nb][2] = acc[h][mt][nb][3] = 0.f;
   const uint4 z = make_uint4(0u, 0u, 0u, 0u);
   // every ancestor's panel descriptor at once (lane l - 1 holds level l's),
   // instead of a chain of dependent loads per level
@@ -487,27 +531,33 @@ __global__ void __launch_bounds__(32 * kP2Warps, kP2PerSm / kP2Warps) k_mx_p2(in
       const uint4 h1 = two ? __ldcs(uh + (ct + 1) * 32) : z;
       const uint4 l0 = __ldcs(ul + ct * 32);
       const uint4 l1 = two ? __ldcs(ul + (ct + 1) * 32) : z;
-      const uint4 t0 = __ldg(tl + ct * 32);
-      const uint4 t1 = two ? __ldg(tl + (ct + 1) * 32) : z;
-      // B pairs {T[2t], T[2t+1]} per tile from the per-column {hi, lo} words
-      const uint32_t bh[2][2] = {{__byte_perm(t0.x, t0.z, 0x5410), __byte_perm(t1.x, t1.z, 0x5410)},
-                                 {__byte_perm(t0.y, t0.w, 0x5410), __byte_perm(t1.y, t1.w, 0x5410)}};
-      const uint32_t bl[2][2] = {{__byte_perm(t0.x, t0.z, 0x7632), __byte_perm(t1.x, t1.z, 0x7632)},
-                                 {__byte_perm(t0.y, t0.w, 0x7632), __byte_perm(t1.y, t1.w, 0x7632)}};
-      mx_p2_step(acc, h0, h1, l0, l1, bh, bl, true);
+#pragma unroll
+      for (int h = 0; h < NH; ++h) {
+        const uint4 t0 = __ldg(tl + h * (th >> 2) + ct * 32);
+        const uint4 t1 = two ? __ldg(tl + h * (th >> 2) + (ct + 1) * 32) : z;
+        // B pairs {T[2t], T[2t+1]} per tile from the per-column {hi, lo} words
+        const uint32_t bh[2][2] = {{__byte_perm(t0.x, t0.z, 0x5410), __byte_perm(t1.x, t1.z, 0x5410)},
+                                   {__byte_perm(t0.y, t0.w, 0x5410), __byte_perm(t1.y, t1.w, 0x5410)}};
+        const uint32_t bl[2][2] = {{__byte_perm(t0.x, t0.z, 0x7632), __byte_perm(t1.x, t1.z, 0x7632)},
+                                   {__byte_perm(t0.y, t0.w, 0x7632), __byte_perm(t1.y, t1.w, 0x7632)}};
+        mx_p2_step(acc[h], h0, h1, l0, l1, bh, bl, true);
+      }
     }
     // tiles without: U_hi T_hi
-    const uint2* th = reinterpret_cast<const uint2*>(T + ot + (long long)nctl * 128) + lane;
+    const uint2* tw = reinterpret_cast<const uint2*>(T + ot + (long long)nctl * 128) + lane;
 #pragma unroll 2
     for (int ct = nctl; ct < nct; ct += 2) {
       const bool two = ct + 1 < nct;
       const uint4 h0 = __ldcs(uh + ct * 32);
       const uint4 h1 = two ? __ldcs(uh + (ct + 1) * 32) : z;
-      const uint2 w0 = __ldg(th + (ct - nctl) * 32);
-      const uint2 w1 = two ? __ldg(th + (ct - nctl + 1) * 32) : make_uint2(0u, 0u);
-      const uint32_t bh[2][2] = {{__byte_perm(w0.x, w0.y, 0x5410), __byte_perm(w1.x, w1.y, 0x5410)},
-                                 {__byte_perm(w0.x, w0.y, 0x7632), __byte_perm(w1.x, w1.y, 0x7632)}};
-      mx_p2_step_hi(acc, h0, h1, bh);
+#pragma unroll
+      for (int h = 0; h < NH; ++h) {
+        const uint2 w0 = __ldg(tw + h * (th >> 1) + (ct - nctl) * 32);
+        const uint2 w1 = two ? __ldg(tw + h * (th >> 1) + (ct - nctl + 1) * 32) : make_uint2(0u, 0u);
+        const uint32_t bh[2][2] = {{__byte_perm(w0.x, w0.y, 0x5410), __byte_perm(w1.x, w1.y, 0x5410)},
+                                   {__byte_perm(w0.x, w0.y, 0x7632), __byte_perm(w1.x, w1.y, 0x7632)}};
+        mx_p2_step_hi(acc[h], h0, h1, bh);
+      }
     }
   }
   for (int q = leaf_dptr[x]; q < leaf_dptr[x + 1]; ++q) {
@@ -519,28 +569,33 @@ __global__ void __launch_bounds__(32 * kP2Warps, kP2PerSm / kP2Warps) k_mx_p2(in
       const uint4 h0 = __ldcs(dh + ct * 32), h1 = __ldcs(dh + (ct + 1) * 32);
       const uint4 l0 = __ldcs(dl + ct * 32), l1 = __ldcs(dl + (ct + 1) * 32);
       const size_t xt = (size_t)(D.col_tile0 + (ct >> 2)) * 128 + (size_t)((ct >> 1) & 1) * 32 + lane;
-      const uint4 xh = __ldg(Xf + xt), xl = __ldg(Xf + xt + 64);
-      const uint32_t bh[2][2] = {{xh.x, xh.z}, {xh.y, xh.w}};
-      const uint32_t bl[2][2] = {{xl.x, xl.z}, {xl.y, xl.w}};
-      mx_p2_step(acc, h0, h1, l0, l1, bh, bl, true);
+#pragma unroll
+      for (int h = 0; h < NH; ++h) {
+        const uint4 xh = __ldg(Xf + h * xh_ + xt), xl = __ldg(Xf + h * xh_ + xt + 64);
+        const uint32_t bh[2][2] = {{xh.x, xh.z}, {xh.y, xh.w}};
+        const uint32_t bl[2][2] = {{xl.x, xl.z}, {xl.y, xl.w}};
+        mx_p2_step(acc[h], h0, h1, l0, l1, bh, bl, true);
+      }
     }
   }
   const int base = leaf_off[x] + 32 * (G - leaf_tile0[x]);
   const int lim = leaf_off[x + 1];
 #pragma unroll
-  for (int mt = 0; mt < 2; ++mt)
+  for (int h = 0; h < NH; ++h)
 #pragma unroll
-    for (int nb = 0; nb < 2; ++nb) {
-      const int ra = base + 16 * mt + g, rb = ra + 8, c = 8 * nb + 2 * t;
-      if (c < nr) {
-        if (ra < lim) Y[(size_t)c * ldy + ra] = acc[mt][nb][0];
-        if (rb < lim) Y[(size_t)c * ldy + rb] = acc[mt][nb][2];
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nb = 0; nb < 2; ++nb) {
+        const int ra = base + 16 * mt + g, rb = ra + 8, c = 16 * h + 8 * nb + 2 * t;
+        if (c < nr) {
+          if (ra < lim) Y[(size_t)c * ldy + ra] = acc[h][mt][nb][0];
+          if (rb < lim) Y[(size_t)c * ldy + rb] = acc[h][mt][nb][2];
+        }
+        if (c + 1 < nr) {
+          if (ra < lim) Y[(size_t)(c + 1) * ldy + ra] = acc[h][mt][nb][1];
+          if (rb < lim) Y[(size_t)(c + 1) * ldy + rb] = acc[h][mt][nb][3];
+        }
       }
-      if (c + 1 < nr) {
-        if (ra < lim) Y[(size_t)(c + 1) * ldy + ra] = acc[mt][nb][1];
-        if (rb < lim) Y[(size_t)(c + 1) * ldy + rb] = acc[mt][nb][3];
-      }
-    }
 }
 
 // ---- conversion (build time) ------------------------------------------------
@@ -915,44 +970,60 @@ hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, int 
 hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, float* scratch,
                           cudaStream_t s, KernelMarks* km) {
   MxPlan& M = h->mx;
+  if (nr < 1 || nr > 32) return fail(HM_ERR_INVALID, "mixed product: a pass holds 1 to 32 right-hand sides");
+  const int nh = nr > 16 ? 2 : 1;  // halves of 16 right-hand sides in this pass
+  // scratch: the halves' X fragments, then their chunk partials, then their T
+  const long long xh = (long long)M.num_tiles * 128, sh = M.s_tiles * 32, th = M.t_words;
   uint4* Xf = reinterpret_cast<uint4*>(scratch);
-  float4* S = reinterpret_cast<float4*>(scratch + (size_t)M.num_tiles * 4 * 128);
-  uint32_t* T = reinterpret_cast<uint32_t*>(S + (size_t)M.s_tiles * 32);
+  float4* S = reinterpret_cast<float4*>(Xf + nh * xh);
+  uint32_t* T = reinterpret_cast<uint32_t*>(S + nh * sh);
   const int* leaf_off = h->tree->offsets.p;
+  const long long xbytes = 4ll * h->n * 16 * nh;  // the X fragments, hi + lo
   if (M.num_tiles > 0) {
-    k_mx_split_x<<<(M.num_tiles + 3) / 4, 128, 0, s>>>(X, ldx, nr, M.num_tiles, M.tile_leaf.p, M.leaf_tile0.p,
-                                                       leaf_off, Xf);
+    k_mx_split_x<<<dim3((M.num_tiles + 3) / 4, nh), 128, 0, s>>>(X, ldx, nr, M.num_tiles, M.tile_leaf.p,
+                                                                 M.leaf_tile0.p, leaf_off, Xf);
     HM_LAUNCH_CHECK();
-    if (km) km->mark("k_mx_split_x", 4ll * h->n * nr + 4ll * h->n * 16, s);
+    if (km) km->mark("k_mx_split_x", 4ll * h->n * nr + xbytes, s);
   }
   if (M.num_units > 0) {
-    if (M.p1_ring && M.group_tiles <= 4) {
+    if (M.p1_ring && nh == 1 && M.group_tiles <= 4) {
       k_mx_p1r<8, 3, 4><<<M.num_sms, 256, ring_smem<8, 3, 4>(), s>>>(M.units.p, M.num_units, M.panels.p, M.store.p,
                                                                       Xf, M.tslot.p, S, T);
-    } else if (M.p1_ring) {
+    } else if (M.p1_ring && nh == 1) {
       k_mx_p1r<4, 4, 8><<<M.num_sms, 128, ring_smem<4, 4, 8>(), s>>>(M.units.p, M.num_units, M.panels.p, M.store.p,
                                                                       Xf, M.tslot.p, S, T);
+    } else if (nh == 1) {
+      k_mx_p1<1><<<(M.num_units + kP1Warps - 1) / kP1Warps, 32 * kP1Warps, 0, s>>>(
+          M.units.p, M.num_units, M.panels.p, M.store.p, Xf, M.tslot.p, S, T, xh, sh, th);
     } else {
-      k_mx_p1<<<(M.num_units + kP1Warps - 1) / kP1Warps, 32 * kP1Warps, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf,
-                                                    M.tslot.p, S, T);
+      k_mx_p1<2><<<(M.num_units + kP1Warps - 1) / kP1Warps, 32 * kP1Warps, 0, s>>>(
+          M.units.p, M.num_units, M.panels.p, M.store.p, Xf, M.tslot.p, S, T, xh, sh, th);
     }
     HM_LAUNCH_CHECK();
-    if (km) km->mark("k_mx_p1", M.bytes_p1 + 4ll * h->n * 16, s);
+    if (km) km->mark("k_mx_p1", M.bytes_p1 + xbytes, s);
   }
   if (M.nmt > 0) {
-    k_mx_reduce<<<(unsigned)((M.nmt * 32 + 255) / 256), 256, 0, s>>>(M.mtiles.p, M.nmt, M.panels.p, S,
-                                                                      M.tslot.p, T);
+    k_mx_reduce<<<dim3((unsigned)((M.nmt * 32 + 255) / 256), nh), 256, 0, s>>>(M.mtiles.p, M.nmt, M.panels.p, S,
+                                                                               M.tslot.p, T, sh, th);
     HM_LAUNCH_CHECK();
-    if (km) km->mark("k_mx_reduce", 512ll * M.s_tiles + 512ll * M.nmt, s);
+    if (km) km->mark("k_mx_reduce", (512ll * M.s_tiles + 512ll * M.nmt) * nh, s);
   }
   if (M.num_tiles > 0) {
-    k_mx_p2<<<(M.num_tiles + kP2Warps - 1) / kP2Warps, 32 * kP2Warps, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
-                                                  M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p,
-                                                  M.leaf_dblk.p, M.dense.p, Xf, Y, ldy, nr);
+    const unsigned grid = (unsigned)((M.num_tiles + kP2Warps - 1) / kP2Warps);
+    if (nh == 1)
+      k_mx_p2<1><<<grid, 32 * kP2Warps, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
+                                                M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p, M.leaf_dblk.p,
+                                                M.dense.p, Xf, Y, ldy, nr, xh, th);
+    else
+      k_mx_p2<2><<<grid, 32 * kP2Warps, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
+                                                M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p, M.leaf_dblk.p,
+                                                M.dense.p, Xf, Y, ldy, nr, xh, th);
     HM_LAUNCH_CHECK();
-    if (km) km->mark("k_mx_p2", M.bytes_p2 + 4ll * h->n * 16 + 4ll * h->n * nr, s);
+    if (km) km->mark("k_mx_p2", M.bytes_p2 + xbytes + 4ll * h->n * nr, s);
   }
-  if (h->diag_fly) HM_TRY(diag_fly_panel(h, nr, X, ldx, Y, ldy, s, km));
+  if (h->diag_fly)  // the diagonal from coordinates, 16 columns at a time
+    for (int c0 = 0; c0 < nr; c0 += 16)
+      HM_TRY(diag_fly_panel(h, std::min(16, nr - c0), X + (size_t)c0 * ldx, ldx, Y + (size_t)c0 * ldy, ldy, s, km));
   return HM_OK;
 }
 

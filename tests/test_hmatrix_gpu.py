@@ -244,3 +244,29 @@ def test_mixed_moves_fewer_bytes_and_agrees_with_fp32(hm):
     rel = (torch.linalg.norm(Ym - Yf) / torch.linalg.norm(Yf)).item()
     assert rel < 1e-4, rel
     assert _profile_bytes(hm, Hm, n) < 0.8 * _profile_bytes(hm, Hf, n)
+
+
+@pytest.mark.parametrize("diag_from_coords", [0, 1])
+def test_mixed_two_half_passes_match_single_passes(hm, diag_from_coords):
+    """The mixed form multiplies up to 32 right-hand sides per pass: two halves
+    of 16 share every factor tile read.  A 40-column product (a pass of 32 and
+    one of 8) equals the same columns multiplied 16, 16 and 8 at a time, in
+    tree order and in the points' original order, with the diagonal blocks
+    stored or generated from coordinates."""
+    import torch
+
+    n, d, b = 24000, 3, 64
+    kind, ell, nugget, tol = hm.K_MATERN32, 0.2, 1e-3, 1e-4
+    pts = hm.generate_dataset(n, d, seed=31)
+    tree = hm.construct_kdtree(pts, n, d, b)
+    st = hm.construct_hmatrix_structure(tree, hm.BOX_CENTER, 1.0)
+    H = hm.build_hmatrix(tree, st, pts, kernel=kind, ell=ell, nugget=nugget, tol=tol, max_rank=128,
+                         precision=hm.PREC_MIXED, diag_from_coords=diag_from_coords)
+    X = torch.randn((40, n), device="cuda", dtype=torch.float32).t()
+    for orig in (False, True):
+        Y = H.matvec(X, original_order=orig)
+        parts = [H.matvec(X[:, c0:c1].t().contiguous().t(), original_order=orig) for c0, c1 in
+                 ((0, 16), (16, 32), (32, 40))]
+        Ys = torch.cat(parts, dim=1)
+        scale = torch.linalg.norm(Ys).item()
+        assert torch.linalg.norm(Y - Ys).item() <= 1e-6 * scale
