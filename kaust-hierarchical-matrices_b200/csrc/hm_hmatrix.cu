@@ -1258,6 +1258,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
     while (pstart < nprob) {
       const long long pend = batch_end[bi++];
       const int nb = (int)(pend - pstart);
+      tr.mark("batch begin", stream, nb);
       std::vector<Prob> bp(probs.begin() + pstart, probs.begin() + pend);
       size_t off = 0;
       std::vector<int2> items_rows, items_cols;
@@ -1367,9 +1368,11 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
           k_kmm<W><<<(unsigned)items_rows.size(), kKmmThreads, kmm_smem<W>(), stream>>>(ka);
         }
         HM_LAUNCH_CHECK();
+        tr.mark("  round sketch", stream, round);
         oa.round = round;
         k_orth<W><<<nb, kOrthThreads, orth_smem<W>(), stream>>>(oa);
         HM_LAUNCH_CHECK();
+        tr.mark("  round orth", stream, round);
         HM_CUDA(cudaMemcpyAsync(hst.data(), dst.p, sizeof(ProbState) * nb, cudaMemcpyDeviceToHost, stream));
         HM_CUDA(cudaStreamSynchronize(stream));
         bool any = false;
@@ -1391,9 +1394,11 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
         }
         if ((st = qt.alloc_async(std::max<size_t>(qw, 1), stream)) || (st = dqpoff.alloc_async(nb, stream)))
           return st;
+        tr.mark("  q table alloc (MB)", stream, (long long)(qw * 16 >> 20));
         HM_CUDA(cudaMemcpyAsync(dqpoff.p, qpoff.data(), sizeof(long long) * nb, cudaMemcpyHostToDevice, stream));
         k_pack_q<<<nb, 256, 0, stream>>>(dprobs.p, dst.p, reinterpret_cast<const float*>(ws.p), dqpoff.p, qt.p);
         HM_LAUNCH_CHECK();
+        tr.mark("  q pack", stream, nb);
         kf.qt = qt.p;
         kf.qpoff = dqpoff.p;
         // one launch per basis-width class, so the narrow (most) blocks run
