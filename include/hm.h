@@ -49,7 +49,8 @@ typedef enum {
   HM_ERR_CUDA = 2,          /* a CUDA runtime call failed */
   HM_ERR_NOMEM = 3,         /* device or host allocation failed */
   HM_ERR_UNSUPPORTED = 4,   /* valid request outside what this build supports */
-  HM_ERR_TIMEOUT = 5        /* a bounded device-side wait gave up */
+  HM_ERR_TIMEOUT = 5,       /* a bounded device-side wait gave up */
+  HM_ERR_NOT_CONVERGED = 6  /* an iterative solve stopped at its iteration limit */
 } hm_status;
 
 typedef enum { HM_ADMISS_WEAK = 0, HM_ADMISS_BOX_CENTER = 1 } hm_admissibility;
@@ -217,6 +218,31 @@ HM_API hm_status hm_hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, i
  * streams, other host threads) race and must be serialised by the caller. */
 HM_API hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, int ldx, float* Y, int ldy,
                                     void* stream);
+
+/* Conjugate gradients on the H-matrix: solves H X = B (tree order, X and B
+ * n x nrhs column-major) for a symmetric positive definite kernel matrix, e.g.
+ * a kernel with a nugget on its diagonal (kernel ridge regression, a
+ * Gaussian-process solve).  No counterpart in the reference, which has no
+ * solver; it is the natural consumer of the product (hm_hmatvec).
+ *
+ * One CG per column, all columns sharing every product; X starts at zero.
+ * Vectors are FP32, dot products FP64 in a fixed order.  The stream's work
+ * is checked every `check_every` iterations: a column is done when
+ * ||r|| <= tol ||b||, the solve when every column is.  On a created stream
+ * each chunk of check_every iterations is recorded once into a CUDA graph and
+ * relaunched; on the legacy stream the iterations are launched directly.
+ * Allocates its workspace (4 n x nrhs floats) from the stream-ordered pool
+ * and synchronises the stream between chunks.  *iterations receives the
+ * iterations run, *rel_residual the worst column's true relative residual
+ * ||B - H X|| / ||B||, recomputed with one more product.  The tolerance is
+ * tested on CG's recurrence; the mixed form's product is linear only to its
+ * BF16 rounding (about 1e-4 relative), so there the true residual levels off
+ * near that however small tol is.  Returns
+ * HM_ERR_NOT_CONVERGED when max_iter iterations do not meet tol (X holds the
+ * last iterate), HM_ERR_UNSUPPORTED when the operator shows itself not
+ * positive definite (p.Ap <= 0). */
+HM_API hm_status hm_cg_solve(hm_hmatrix h, int nrhs, const float* B, int ldb, float* X, int ldx, double tol,
+                             int max_iter, int check_every, void* stream, int* iterations, double* rel_residual);
 
 /* hm_hmatvec for one pass (nrhs <= 16; <= 32 for the mixed form, whose
  * passes multiply two halves of 16 right-hand sides per factor read), X and Y

@@ -109,6 +109,7 @@ def lib():
             L.hm_batch_free.argtypes = [P]
             L.hm_autotune.argtypes = [P, I, ctypes.c_char_p, P, P, ctypes.c_char_p, I]
             L.hm_schedule_set.argtypes = [P, ctypes.c_char_p, P]
+            L.hm_cg_solve.argtypes = [P, I, P, I, P, I, D, I, I, P, P, P]
         _lib = L
     return _lib
 
@@ -116,6 +117,15 @@ def lib():
 def _check(status):
     if status != 0:
         raise HMError(status, lib().hm_last_error().decode())
+
+
+def _check_vectors(X, n, name):
+    """The C ABI takes raw pointers and trusts the sizes it is given: a block
+    of vectors must be a float32 CUDA tensor of shape (n, nrhs)."""
+    if X.dim() != 2 or X.shape[0] != n or X.shape[1] < 1:
+        raise ValueError("%s must have shape (%d, nrhs), got %s" % (name, n, tuple(X.shape)))
+    if str(X.dtype) != "torch.float32" or X.device.type != "cuda":
+        raise ValueError("%s must be a float32 CUDA tensor" % name)
 
 
 def _ptr(t):
@@ -267,11 +277,15 @@ class HMatrix:
         n = self.n
         if X.dim() == 1:
             X = X[:, None]
+        _check_vectors(X, n, "X")
         nrhs = X.shape[1]
         Xc = X.t().contiguous() if not X.t().is_contiguous() else X.t()
         if Y is None:
             Yc = torch.empty((nrhs, n), dtype=torch.float32, device=X.device)
         else:
+            _check_vectors(Y, n, "Y")
+            if Y.shape[1] != nrhs:
+                raise ValueError("Y must have as many columns as X")
             Yc = Y.t()
             assert Yc.is_contiguous()
         _check(lib().hm_hmatvec(self.h, trans, nrhs, _ptr(Xc), n, _ptr(Yc), n, 1 if original_order else 0,
@@ -376,6 +390,26 @@ def autotune(H, nrhs=16, cache_path=None, stream=None):
     _check(lib().hm_autotune(H.h, nrhs, cache_path.encode() if cache_path else None, _stream(stream),
                              ctypes.byref(fc), buf, 128))
     return buf.value.decode(), bool(fc.value)
+
+
+def cg_solve(H, B, tol=1e-6, max_iter=1000, check_every=8, stream=None):
+    """Solve H X = B by conjugate gradients (hm_cg_solve), tree order.  B: a
+    float32 CUDA tensor (n, nrhs) with B.T contiguous, or (n,).  Returns (X,
+    iterations, worst true relative residual); raises HMError with status 6
+    when max_iter iterations do not reach tol."""
+    import torch
+
+    n = H.n
+    if B.dim() == 1:
+        B = B[:, None]
+    _check_vectors(B, n, "B")
+    nrhs = B.shape[1]
+    Bc = B.t().contiguous() if not B.t().is_contiguous() else B.t()
+    Xc = torch.empty((nrhs, n), dtype=torch.float32, device=B.device)
+    it, res = ctypes.c_int(), ctypes.c_double()
+    _check(lib().hm_cg_solve(H.h, nrhs, _ptr(Bc), n, _ptr(Xc), n, tol, max_iter, check_every, _stream(stream),
+                             ctypes.byref(it), ctypes.byref(res)))
+    return Xc.t(), it.value, res.value
 
 
 def schedule_set(H, choice, stream=None):
