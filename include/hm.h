@@ -284,6 +284,22 @@ HM_API hm_status hm_hmatrix_dense_block(hm_hmatrix h, int i, float* D);
 
 HM_API void hm_hmatrix_free(hm_hmatrix h);
 
+/* Binary H-matrix files: build once, apply many times.  No counterpart in the
+ * reference, which only dumps text (src/helperFunctions.cu:76-169).
+ *
+ * hm_hmatrix_save writes the options, every stored low-rank pair (FP32
+ * factors, rank, low-part columns) and dense block, and a fingerprint of the
+ * tree and structure (permutation, leaf offsets, admissibility, block lists);
+ * it synchronises the device.  hm_hmatrix_load reads such a file into a new
+ * H-matrix on `t` and `s`, which must be the tree and structure it was built
+ * on (rebuild them from the same points, bucket and admissibility; a
+ * different one is refused with HM_ERR_INVALID), and rebuilds the product's
+ * plans (and the mixed form's BF16 panels) exactly as the build does: its
+ * products equal the saved matrix's.  A file from another version of the
+ * library, or a damaged one, is refused with HM_ERR_INVALID. */
+HM_API hm_status hm_hmatrix_save(hm_hmatrix h, const char* path);
+HM_API hm_status hm_hmatrix_load(hm_kdtree t, hm_structure s, const char* path, void* stream, hm_hmatrix* out);
+
 /* Schedule autotuner (no counterpart in the reference).  Times the product's
  * schedule candidates on this matrix (nrhs columns, at most one pass of the
  * product: 16, or 32 for the mixed form) and keeps the fastest: for the FP32

@@ -1623,6 +1623,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       b.n = P.n;
       b.U = fu[i];
       b.V = fv[i];
+      b.khi = std::min(rhis[i], rank[i]);
       h->h_lr.push_back(b);
       LRBlock bt = b;
       bt.r0 = P.c0;

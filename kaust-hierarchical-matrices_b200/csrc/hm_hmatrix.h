@@ -35,6 +35,7 @@ hm_status diag_fly_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float
 struct LRBlock {
   int r0, m, c0, n, k;
   int level;
+  int khi;         // leading columns that keep a BF16 low part in the mixed form
   const float* U;  // m x k, column-major (ld m)
   const float* V;  // n x k, column-major (ld n)
   long long toff;  // offset of this block's k x nrhs_max projection in the T workspace

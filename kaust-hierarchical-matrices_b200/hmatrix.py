@@ -110,6 +110,8 @@ def lib():
             L.hm_autotune.argtypes = [P, I, ctypes.c_char_p, P, P, ctypes.c_char_p, I]
             L.hm_schedule_set.argtypes = [P, ctypes.c_char_p, P]
             L.hm_cg_solve.argtypes = [P, I, P, I, P, I, D, I, I, P, P, P]
+            L.hm_hmatrix_save.argtypes = [P, ctypes.c_char_p]
+            L.hm_hmatrix_load.argtypes = [P, P, ctypes.c_char_p, P, ctypes.POINTER(P)]
         _lib = L
     return _lib
 
@@ -264,6 +266,10 @@ class HMatrix:
         self.structure = structure
         self.n = tree.n
 
+    def save(self, path):
+        """Write the H-matrix to a binary file (hm_hmatrix_save)."""
+        _check(lib().hm_hmatrix_save(self.h, str(path).encode()))
+
     def stats(self):
         st = Stats()
         _check(lib().hm_hmatrix_stats_get(self.h, ctypes.byref(st)))
@@ -410,6 +416,14 @@ def cg_solve(H, B, tol=1e-6, max_iter=1000, check_every=8, stream=None):
     _check(lib().hm_cg_solve(H.h, nrhs, _ptr(Bc), n, _ptr(Xc), n, tol, max_iter, check_every, _stream(stream),
                              ctypes.byref(it), ctypes.byref(res)))
     return Xc.t(), it.value, res.value
+
+
+def load_hmatrix(tree, structure, path, stream=None):
+    """Read an H-matrix written by HMatrix.save (hm_hmatrix_load); tree and
+    structure must be the ones it was built on."""
+    h = ctypes.c_void_p()
+    _check(lib().hm_hmatrix_load(tree.h, structure.h, str(path).encode(), _stream(stream), ctypes.byref(h)))
+    return HMatrix(h, tree, structure)
 
 
 def schedule_set(H, choice, stream=None):
