@@ -78,3 +78,41 @@ def test_header_is_plain_c(tmp_path):
     r = subprocess.run(["gcc", "-std=c99", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(src)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_solver_and_file_entry_points_validate_without_gpu(tmp_path):
+    """hm_cg_solve, hm_hmatrix_save and hm_hmatrix_load refuse null handles
+    and bad sizes before any CUDA call."""
+    path = os.path.join(PKG, "libhmb200.so")
+    if not os.path.exists(path):
+        pytest.skip("libhmb200.so not built")
+    lib = ctypes.CDLL(path)
+    lib.hm_last_error.restype = ctypes.c_char_p
+    P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    lib.hm_cg_solve.argtypes = [P, I, P, I, P, I, D, I, I, P, P, P]
+    lib.hm_hmatrix_save.argtypes = [P, ctypes.c_char_p]
+    lib.hm_hmatrix_load.argtypes = [P, P, ctypes.c_char_p, P, ctypes.POINTER(P)]
+    assert lib.hm_cg_solve(None, 1, None, 1, None, 1, 1e-6, 10, 4, None, None, None) == 1
+    assert b"null matrix" in lib.hm_last_error()
+    assert lib.hm_hmatrix_save(None, str(tmp_path / "x.hmb").encode()) == 1
+    out = ctypes.c_void_p()
+    assert lib.hm_hmatrix_load(None, None, b"x", None, ctypes.byref(out)) == 1
+    assert out.value is None
+    assert lib.hm_hmatrix_load(None, None, b"x", None, None) == 1
+
+
+def test_python_wrappers_check_vector_shapes():
+    """The C ABI trusts the sizes it is given; the Python wrappers check a
+    block of vectors (float32 CUDA tensor, shape (n, nrhs)) before calling it."""
+    import torch
+
+    import hmatrix
+
+    with pytest.raises(ValueError, match="shape"):
+        hmatrix._check_vectors(torch.zeros((3, 100)), 100, "B")  # (nrhs, n) by mistake
+    with pytest.raises(ValueError, match="shape"):
+        hmatrix._check_vectors(torch.zeros((100, 0)), 100, "B")
+    with pytest.raises(ValueError, match="float32 CUDA"):
+        hmatrix._check_vectors(torch.zeros((100, 3)), 100, "B")  # a host tensor
+    with pytest.raises(ValueError, match="float32 CUDA"):
+        hmatrix._check_vectors(torch.zeros((100, 3), dtype=torch.float64), 100, "B")
