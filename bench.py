@@ -449,6 +449,34 @@ def run_ours(args):
 
     e2e_ms = CopyPipeline(torch, stream, Xh, (nrhs, n), e2e_product).time(args.warmup, args.steps, barrier, world)
 
+    # ---- optional: conjugate-gradient iterations on the same matrix ----------
+    # (a tolerance no residual meets, so exactly cg_iters iterations run and
+    # the call reports HM_ERR_NOT_CONVERGED, or HM_ERR_UNSUPPORTED if the
+    # compressed operator shows itself indefinite first; device time with CUDA
+    # events on the solve's stream)
+    cg = None
+    if args.cg_iters > 0:
+        cs = torch.cuda.Stream(device=dev)
+        Xs = torch.empty_like(X)
+        it, res_c = ctypes.c_int(), ctypes.c_double()
+
+        def cg_run(k):
+            st_ = lib.hm_cg_solve(Hs[head].h, nrhs, hm._ptr(X), n, hm._ptr(Xs), n, 1e-300, k, 8, hm._stream(cs),
+                                  ctypes.byref(it), ctypes.byref(res_c))
+            if st_ not in (0, 4, 6):
+                hm._check(st_)
+
+        torch.cuda.synchronize()
+        cg_run(16)  # warm-up (records its graph, allocates the workspace from the pool)
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(cs)
+        cg_run(args.cg_iters)
+        c1.record(cs)
+        torch.cuda.synchronize()
+        cg_ms = c0.elapsed_time(c1)
+        cg = {"iterations": it.value, "ms": cg_ms, "ms_per_iteration": cg_ms / max(it.value, 1),
+              "product_ms": res[head]["ms"], "check_every": 8}
+
     # ---- accuracy against the FP64 oracle on sampled rows -------------------
     errs = {}
     if rank == 0 and not args.skip_check:
@@ -492,6 +520,8 @@ def run_ours(args):
             "gpu_launches": r["launches_per_step"] * args.steps,
             "clocks": clocks.summary(local),
         }
+        if cg is not None:
+            line["cg"] = cg
         if "fp32" in res and head != "fp32":
             f = res["fp32"]
             line["fp32_form"] = {
@@ -701,6 +731,9 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=5.0)
+    ap.add_argument("--cg-iters", type=int, default=0,
+                    help="also run this many conjugate-gradient iterations (hm_cg_solve, graph-launched "
+                         "chunks of 8 on a created stream) with the headline form and report ms per iteration")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

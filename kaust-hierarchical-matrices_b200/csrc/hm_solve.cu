@@ -248,6 +248,7 @@ extern "C" hm_status hm_cg_solve(hm_hmatrix h, int nrhs, const float* B, int ldb
     if (st == HM_OK) st = converged();
     if (st == HM_OK && hflag) {
       drop_graph();
+      if (iterations) *iterations = it;
       return fail(HM_ERR_UNSUPPORTED,
                   "hm_cg_solve: p.Ap <= 0 after " + std::to_string(it) +
                       " iterations: the H-matrix is not positive definite (add a nugget, or tighten the "
