@@ -244,8 +244,8 @@ HM_API hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, int 
 HM_API hm_status hm_cg_solve(hm_hmatrix h, int nrhs, const float* B, int ldb, float* X, int ldx, double tol,
                              int max_iter, int check_every, void* stream, int* iterations, double* rel_residual);
 
-/* hm_hmatvec for one pass (nrhs <= 16; <= 32 for the mixed form, whose
- * passes multiply two halves of 16 right-hand sides per factor read), X and Y
+/* hm_hmatvec for one pass (nrhs <= 16; <= 64 for the mixed form, whose
+ * passes multiply up to four parts of 16 right-hand sides per factor read), X and Y
  * in tree order, with CUDA events recorded on `stream`
  * around its two kernels; synchronises and returns each kernel's device time
  * and algorithmic bytes (stored factors and dense blocks read once, X read,
@@ -302,7 +302,7 @@ HM_API hm_status hm_hmatrix_load(hm_kdtree t, hm_structure s, const char* path, 
 
 /* Schedule autotuner (no counterpart in the reference).  Times the product's
  * schedule candidates on this matrix (nrhs columns, at most one pass of the
- * product: 16, or 32 for the mixed form) and keeps the fastest: for the FP32
+ * product: 16, or 64 for the mixed form) and keeps the fastest: for the FP32
  * form the rows of V per phase-1 item, for the mixed form the phase-1 unit
  * shape.  With cache_path set, the choice is appended
  * to that text file under a key of the GPU and the matrix's shape, and a

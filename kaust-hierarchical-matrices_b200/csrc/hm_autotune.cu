@@ -85,7 +85,7 @@ extern "C" hm_status hm_autotune(hm_hmatrix h, int nrhs, const char* cache_path,
   using namespace hm;
   if (!h) return fail(HM_ERR_INVALID, "hm_autotune: null matrix");
   if (nrhs < 1 || nrhs > pass_width(h))
-    return fail(HM_ERR_INVALID, "hm_autotune: need 1 <= nrhs <= one pass of the product (16, or 32 for the mixed form)");
+    return fail(HM_ERR_INVALID, "hm_autotune: need 1 <= nrhs <= one pass of the product (16, or 64 for the mixed form)");
   cudaStream_t s = as_stream(stream);
   const std::string key = shape_key(h, nrhs);
   Choice best;

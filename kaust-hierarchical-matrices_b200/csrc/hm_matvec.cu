@@ -36,8 +36,8 @@ static __device__ __align__(256) float hm_noalloc_scratch[size_t(4) << 20];
 namespace hm {
 
 // Right-hand sides per pass of the product: the mixed form reads every factor
-// tile once for up to two halves of 16, the FP32 form runs 16 at a time.
-int pass_width(hm_hmatrix h) { return h->mx.enabled ? 32 : 16; }
+// tile once for up to four parts of 16, the FP32 form runs 16 at a time.
+int pass_width(hm_hmatrix h) { return h->mx.enabled ? 64 : 16; }
 
 namespace {
 
@@ -461,8 +461,8 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   HM_TRY(P.leaf_dptr.alloc(nleaf + 1));
   HM_TRY(P.leaf_dblk.alloc(dblk.size()));
   // projection scratch of one pass, for whichever form runs (the mixed form
-  // runs passes of up to 32 right-hand sides, the FP32 form 16)
-  const long long scratch = h->mx.enabled ? h->mx.scratch_floats(2) : tk + part;
+  // runs passes of up to 64 right-hand sides, the FP32 form 16)
+  const long long scratch = h->mx.enabled ? h->mx.scratch_floats(4) : tk + part;
   HM_TRY(P.T.alloc(std::max<long long>(scratch, 1)));
   HM_TRY(P.Xp.alloc((size_t)h->n * pass_width(h)));
   HM_TRY(P.Yp.alloc((size_t)h->n * pass_width(h)));
@@ -630,7 +630,7 @@ extern "C" hm_status hm_hmatvec_profile(hm_hmatrix h, int nrhs, const float* X, 
                                         long long* bytes_project, long long* bytes_expand) {
   if (!h) return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: null matrix");
   if (nrhs < 1 || nrhs > hm::pass_width(h) || !X || !Y || ldx < h->n || ldy < h->n)
-    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: need 1 <= nrhs <= one pass (16, or 32 for the mixed "
+    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: need 1 <= nrhs <= one pass (16, or 64 for the mixed "
                                     "form) and valid vectors");
   cudaStream_t s = hm::as_stream(stream);
   hm::KernelMarks km;
@@ -656,7 +656,7 @@ extern "C" hm_status hm_hmatvec_kernels(hm_hmatrix h, int nrhs, const float* X, 
                                         int* count) {
   if (!h) return hm::fail(HM_ERR_INVALID, "hm_hmatvec_kernels: null matrix");
   if (nrhs < 1 || nrhs > hm::pass_width(h) || !X || !Y || ldx < h->n || ldy < h->n || cap < 0)
-    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_kernels: need 1 <= nrhs <= one pass (16, or 32 for the mixed "
+    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_kernels: need 1 <= nrhs <= one pass (16, or 64 for the mixed "
                                     "form) and valid vectors");
   hm::KernelMarks km;
   HM_TRY(hm::timed_panel(h, nrhs, X, ldx, Y, ldy, hm::as_stream(stream), &km));

@@ -253,6 +253,13 @@ __global__ void __launch_bounds__(32 * kP1Warps, kP1PerSm / kP1Warps) k_mx_p1(co
       mx_p1_unit<4, 2, 1>(u, P, store, Xf, tslot, S, T, xh, sh, th, lane);
     else
       mx_p1_unit<2, 4, 1>(u, P, store, Xf, tslot, S, T, xh, sh, th, lane);
+  } else if (NH == 4) {  // four halves: two column tiles at a time
+    for (int c = 0; c < u.nct; c += 2) {
+      MxUnit a = u;
+      a.ct0 = u.ct0 + c;
+      a.nct = min(2, u.nct - c);
+      mx_p1_unit<2, 1, NH>(a, P, store, Xf, tslot, S, T, xh, sh, th, lane);
+    }
   } else if (u.nct > 2) {  // two halves: at most four column tiles at a time
     MxUnit a = u;
     a.nct = min(u.nct, 4);
@@ -469,8 +476,9 @@ __device__ __forceinline__ void mx_p2_step_hi(float (&acc)[2][2][4], const uint4
 // panel rows times its T, then the dense blocks of the leaf row.
 // (one warp per CTA, 28 per SM, measured: the kernel is bound by loads in
 // flight, and a warp that finishes its row tile frees its slot at once)
-// With two halves of 16 right-hand sides every U tile is loaded once for both,
-// and the warp holds twice the accumulators (16 warps per SM, 128 registers).
+// With two or four halves of 16 right-hand sides every U tile is loaded once
+// for all of them, and the warp holds their accumulators (16 warps per SM,
+// 128 registers).
 constexpr int kP2Warps = 1, kP2PerSm = 28, kP2PerSm2 = 16;
 template <int NH>
 __global__ void __launch_bounds__(32 * kP2Warps, (NH == 1 ? kP2PerSm : kP2PerSm2) / kP2Warps)
@@ -970,8 +978,10 @@ hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, int 
 hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, float* scratch,
                           cudaStream_t s, KernelMarks* km) {
   MxPlan& M = h->mx;
-  if (nr < 1 || nr > 32) return fail(HM_ERR_INVALID, "mixed product: a pass holds 1 to 32 right-hand sides");
-  const int nh = nr > 16 ? 2 : 1;  // halves of 16 right-hand sides in this pass
+  if (nr < 1 || nr > 64) return fail(HM_ERR_INVALID, "mixed product: a pass holds 1 to 64 right-hand sides");
+  // 16-column parts of this pass: 1, 2 or 4 (a pass of 33-48 runs four, the
+  // last one zero)
+  const int nh = nr > 32 ? 4 : (nr > 16 ? 2 : 1);
   // scratch: the halves' X fragments, then their chunk partials, then their T
   const long long xh = (long long)M.num_tiles * 128, sh = M.s_tiles * 32, th = M.t_words;
   uint4* Xf = reinterpret_cast<uint4*>(scratch);
@@ -995,8 +1005,11 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
     } else if (nh == 1) {
       k_mx_p1<1><<<(M.num_units + kP1Warps - 1) / kP1Warps, 32 * kP1Warps, 0, s>>>(
           M.units.p, M.num_units, M.panels.p, M.store.p, Xf, M.tslot.p, S, T, xh, sh, th);
-    } else {
+    } else if (nh == 2) {
       k_mx_p1<2><<<(M.num_units + kP1Warps - 1) / kP1Warps, 32 * kP1Warps, 0, s>>>(
+          M.units.p, M.num_units, M.panels.p, M.store.p, Xf, M.tslot.p, S, T, xh, sh, th);
+    } else {
+      k_mx_p1<4><<<(M.num_units + kP1Warps - 1) / kP1Warps, 32 * kP1Warps, 0, s>>>(
           M.units.p, M.num_units, M.panels.p, M.store.p, Xf, M.tslot.p, S, T, xh, sh, th);
     }
     HM_LAUNCH_CHECK();
@@ -1014,8 +1027,12 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
       k_mx_p2<1><<<grid, 32 * kP2Warps, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
                                                 M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p, M.leaf_dblk.p,
                                                 M.dense.p, Xf, Y, ldy, nr, xh, th);
-    else
+    else if (nh == 2)
       k_mx_p2<2><<<grid, 32 * kP2Warps, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
+                                                M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p, M.leaf_dblk.p,
+                                                M.dense.p, Xf, Y, ldy, nr, xh, th);
+    else
+      k_mx_p2<4><<<grid, 32 * kP2Warps, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
                                                 M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p, M.leaf_dblk.p,
                                                 M.dense.p, Xf, Y, ldy, nr, xh, th);
     HM_LAUNCH_CHECK();

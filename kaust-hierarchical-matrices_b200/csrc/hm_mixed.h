@@ -87,7 +87,7 @@ struct MxPlan {
   // scratch of one 16-column panel of right-hand sides, in floats: X
   // fragments, chunk partials, T (the projections by expanding column: BF16
   // hi + lo for the columns with low parts, hi for the others)
-  // of a pass of `halves` such panels (1 or 2: up to 32 right-hand sides)
+  // of a pass of `halves` such panels (1, 2 or 4: up to 64 right-hand sides)
   long long scratch_floats(int halves = 1) const {
     return (((long long)num_tiles * 4 + s_tiles) * 128 + t_words) * halves;
   }
@@ -117,9 +117,9 @@ struct KernelMarks;
 // matvec plan afterwards (the scratch size changes).
 hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, int p1_ring, cudaStream_t s);
 
-// One pass of nr <= 32 right-hand sides in tree order (two halves of 16 when
-// nr > 16: every factor tile is read once for both); scratch holds
-// scratch_floats(nr > 16 ? 2 : 1) floats.  km (optional) receives an event
+// One pass of nr <= 64 right-hand sides in tree order (two or four parts of 16
+// when nr > 16: every factor tile is read once for all of them); scratch holds
+// scratch_floats(h) floats, h = 1, 2 or 4 parts.  km (optional) receives an event
 // after each kernel.
 hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, float* scratch,
                           cudaStream_t s, KernelMarks* km);
