@@ -476,9 +476,8 @@ __device__ __forceinline__ void mx_p2_step_hi(float (&acc)[2][2][4], const uint4
 // panel rows times its T, then the dense blocks of the leaf row.
 // (one warp per CTA, 28 per SM, measured: the kernel is bound by loads in
 // flight, and a warp that finishes its row tile frees its slot at once)
-// With two or four halves of 16 right-hand sides every U tile is loaded once
-// for all of them, and the warp holds their accumulators (16 warps per SM,
-// 128 registers).
+// With two halves of 16 right-hand sides every U tile is loaded once for both,
+// and the warp holds twice the accumulators (16 warps per SM, 128 registers).
 constexpr int kP2Warps = 1, kP2PerSm = 28, kP2PerSm2 = 16;
 template <int NH>
 __global__ void __launch_bounds__(32 * kP2Warps, (NH == 1 ? kP2PerSm : kP2PerSm2) / kP2Warps)
@@ -1031,10 +1030,13 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
       k_mx_p2<2><<<grid, 32 * kP2Warps, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
                                                 M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p, M.leaf_dblk.p,
                                                 M.dense.p, Xf, Y, ldy, nr, xh, th);
-    else
-      k_mx_p2<4><<<grid, 32 * kP2Warps, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
-                                                M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p, M.leaf_dblk.p,
-                                                M.dense.p, Xf, Y, ldy, nr, xh, th);
+    else  // four parts: two launches of two parts each (a four-part phase 2 spills
+          // at 128 registers and measured slower than two of these)
+      for (int q = 0; q < 2 && nr > 32 * q; ++q)
+        k_mx_p2<2><<<grid, 32 * kP2Warps, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
+                                                  M.pan_of.p, M.panels.p, M.store.p, T + 2 * q * th, M.leaf_dptr.p,
+                                                  M.leaf_dblk.p, M.dense.p, Xf + 2 * q * xh, Y + (size_t)32 * q * ldy,
+                                                  ldy, std::min(32, nr - 32 * q), xh, th);
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_mx_p2", M.bytes_p2 + xbytes + 4ll * h->n * nr, s);
   }
