@@ -29,6 +29,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -278,6 +279,14 @@ class CopyPipeline:
         return _ranks.max_over_ranks(t0.elapsed_time(t1) / steps, world)
 
 
+def out_dir():
+    """Where the clock log and the autotuner's cache go: $HM_BENCH_OUT, else
+    the temporary directory."""
+    d = os.environ.get("HM_BENCH_OUT") or tempfile.gettempdir()
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
 def kernel_times(hm, lib, H, X, Y, n, nrhs, stream, reps=6):
     """Per-kernel device times (CUDA events on `stream`) and algorithmic bytes of
     one product, averaged over reps after one warm call."""
@@ -407,8 +416,7 @@ def run_ours(args):
         barrier()
         return ranks.max_over_ranks(t0.elapsed_time(t1) / args.steps, world)
 
-    clocks = ClockSampler(os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % rank)
-                          if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp/bench_clocks_%d.csv" % rank)
+    clocks = ClockSampler(os.path.join(out_dir(), "bench_clocks_%d.csv" % rank))
     res = {}
     for f in forms:
         # the product runs in passes of 64 right-hand sides (mixed form) or 16 (FP32)
@@ -589,8 +597,7 @@ def run_batch(args):
         clouds, front_s = ev_time(front)
         forms = ["mixed", "fp32"] if args.precision == "both" else [args.precision]
         Bs, build_s, tune = {}, {}, {}
-        cache = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp",
-                             "hm_autotune.txt")
+        cache = os.path.join(out_dir(), "hm_autotune.txt")
         for f in forms:
             B = hm.Batch([c[2] for c in clouds], [c[3] for c in clouds], stream=s)
             prec = hm.PREC_MIXED if f == "mixed" else hm.PREC_FP32
@@ -603,8 +610,7 @@ def run_batch(args):
         N = Bs[head].n
         X = torch.randn((nrhs, N), device=dev).t()
         Y = torch.empty((nrhs, N), device=dev).t()
-        clocks = ClockSampler(os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % rank)
-                              if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp/bench_clocks_%d.csv" % rank)
+        clocks = ClockSampler(os.path.join(out_dir(), "bench_clocks_%d.csv" % rank))
         res = {}
         for f in forms:
             B = Bs[f]

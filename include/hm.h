@@ -48,7 +48,7 @@ typedef enum {
   HM_ERR_INVALID = 1,       /* bad argument (null pointer, size, enum) */
   HM_ERR_CUDA = 2,          /* a CUDA runtime call failed */
   HM_ERR_NOMEM = 3,         /* device or host allocation failed */
-  HM_ERR_UNSUPPORTED = 4,   /* valid request outside what this build supports */
+  HM_ERR_UNSUPPORTED = 4,   /* valid request outside what this library supports */
   HM_ERR_TIMEOUT = 5,       /* a bounded device-side wait gave up */
   HM_ERR_NOT_CONVERGED = 6  /* an iterative solve stopped at its iteration limit */
 } hm_status;

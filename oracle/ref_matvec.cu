@@ -1,7 +1,7 @@
 // ref_matvec.cu -- times the reference's own GPU H-matvec (HMatrixVecMult:
 // batched and grouped CUTLASS FP64 GEMMs, src/HMatrixVectorMultiplication.cu)
-// against this engine's hm_hmatvec, on the same H-matrix.  BASELINE
-// MEASUREMENT ONLY (test infrastructure): oracle/Makefile compiles it with the
+// against this engine's hm_hmatvec, on the same H-matrix.  Baseline
+// measurement only (test infrastructure): oracle/Makefile compiles it with the
 // unmodified reference sources into oracle/_ref/ref_matvec.
 //
 // The reference product needs weak admissibility, N / bucket and nrhs powers
