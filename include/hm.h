@@ -102,6 +102,26 @@ HM_API hm_status hm_generate_mixture(int n, int d, int ncomp, double sigma_min, 
 HM_API hm_status hm_kdtree_build(const double* d_points, int n, int d, int bucket, void* stream,
                           hm_kdtree* out);
 
+/* The reference's DIVISION_METHOD (src/config.h:48-52, same values). */
+typedef enum {
+  HM_DIV_POWER_OF_TWO_ON_LEFT = 0,
+  HM_DIV_DIVIDE_IN_HALF = 1,
+  HM_DIV_FULL_TREE = 2
+} hm_division;
+
+/* allocateKDTree(tree, N, d, b, divMethod) + constructKDTree(N, d, b, tree,
+ * points, divMethod) (src/kDTree.cu:6-31, src/kDTreeConstruction.cu:14-231)
+ * with the reference's division argument.  FULL_TREE and DIVIDE_IN_HALF run
+ * the same construction in the reference (they differ only in how many
+ * segment offsets allocateKDTree reserves, src/kDTree.cu:17-22) and give
+ * hm_kdtree_build's tree.  POWER_OF_TWO_ON_LEFT splits segments at
+ * power-of-two offsets (src/kDTreeConstruction.cu:77-206); for a power-of-two
+ * n every such split is the ceil(len/2) split, so the tree is again
+ * hm_kdtree_build's; other n return HM_ERR_UNSUPPORTED.  Any other value is
+ * HM_ERR_INVALID. */
+HM_API hm_status hm_kdtree_build_div(const double* d_points, int n, int d, int bucket, int division,
+                                     void* stream, hm_kdtree* out);
+
 /* depth = number of levels below the root; leaves = 2^depth. */
 HM_API hm_status hm_kdtree_info(hm_kdtree t, int* n, int* d, int* bucket, int* depth);
 
@@ -176,6 +196,20 @@ HM_API void hm_build_opts_default(int d, hm_build_opts* opts);
 HM_API hm_status hm_hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points,
                            const hm_build_opts* opts, void* stream, hm_hmatrix* out);
 
+/* One block-row shard of the H-matrix, for a product spread over several
+ * GPUs (no counterpart in the reference, which runs on one GPU).  The shard
+ * owns the rows of leaves [leaf_begin, leaf_end) -- for G ranks, a contiguous
+ * run of the 2^L subtrees at tree level L = ceil(log2 G) -- and compresses
+ * only the blocks whose row or column cluster overlaps those rows (a pair
+ * across two shards is compressed by both), plus its own diagonal leaves.
+ * Its product (hm_hmatvec, hm_hmatvec_f64) reads all of X and writes only
+ * the shard's rows of Y: the other rows are left untouched.  Stacking the
+ * shards' rows gives the whole matrix's product.  Same tree, structure and
+ * options as hm_hmatrix_build; a shard cannot be saved to a file. */
+HM_API hm_status hm_hmatrix_build_rows(hm_kdtree t, hm_structure s, const double* d_points,
+                                       const hm_build_opts* opts, int leaf_begin, int leaf_end, void* stream,
+                                       hm_hmatrix* out);
+
 typedef struct {
   long long num_lowrank;     /* low-rank blocks (each stored pair counted twice) */
   long long num_dense;       /* dense blocks, diagonal leaves included */
@@ -183,10 +217,15 @@ typedef struct {
   int max_rank_seen;
   long long factor_bytes;    /* bytes of stored factors */
   long long dense_bytes;     /* bytes of stored dense blocks */
-  long long num_unconverged; /* blocks above the leaf level left at their rank cap */
+  long long num_unconverged; /* low-rank blocks stored above the tolerance (none: a block that misses it
+                                at its rank cap is split, see num_split) */
   long long mixed_bytes;     /* mixed form: bytes one product reads from the BF16 copies
                                 (2 B per high part, 2 B per low part, both orientations) */
   double build_seconds;      /* device time of hm_hmatrix_build */
+  long long num_split;       /* admissible blocks that missed the tolerance at their rank cap and were
+                                compressed as their four child blocks instead (recursively; at the
+                                leaf level such a block is stored dense) */
+  long long device_bytes;    /* device memory the matrix holds now (factors, panels, plans, workspaces) */
 } hm_hmatrix_stats;
 
 HM_API hm_status hm_hmatrix_stats_get(hm_hmatrix h, hm_hmatrix_stats* st);
@@ -199,6 +238,19 @@ HM_API hm_status hm_hmatrix_stats_get(hm_hmatrix h, hm_hmatrix_stats* st);
 HM_API hm_status hm_hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, int ldx, float* Y,
                      int ldy, int original_order, void* stream);
 
+/* HMatrixVecMult with the reference's FP64 vectors
+ * (src/HMatrixVectorMultiplication.cu:10, H2Opus_Real = double,
+ * src/precision.h:6): Y = H X (trans = 0) or H^T X (trans = 1) for X, Y
+ * device, column-major n x nrhs FP64 with leading dimensions ldx, ldy >= n.
+ * The library narrows X to FP32 and widens the FP32 result into Y on the
+ * device, a pass of right-hand sides at a time, in the matrix's own per-pass
+ * buffers: no allocation and no host synchronisation.  The arithmetic is the
+ * FP32 or mixed form the matrix was built in, so Y carries that form's error,
+ * not FP64's.  original_order as for hm_hmatvec (the permutation is applied
+ * by the same conversion kernels). */
+HM_API hm_status hm_hmatvec_f64(hm_hmatrix h, int trans, int nrhs, const double* X, int ldx, double* Y, int ldy,
+                                int original_order, void* stream);
+
 /* Allocation-free product.  No counterpart in the reference.
  *
  * Same result as hm_hmatvec(h, 0, nrhs, X, ldx, Y, ldy, 0, stream) (tree
@@ -206,16 +258,29 @@ HM_API hm_status hm_hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, i
  * operator -- code running under an external allocator that owns all device
  * memory, or a latency-bound loop in which a cudaMalloc (which can synchronise
  * the device) is not acceptable.  It allocates nothing and does not use the
- * matrix's own projection workspace: its scratch is one fixed 16 MiB array in
- * the library's device image, held by every GPU that loads the library until
- * the process exits.  Matrices whose projections need more than that
- * (sum of ranks x 16 floats > 4 Mi) are rejected with HM_ERR_UNSUPPORTED.
+ * matrix's own projection workspace: its scratch is one fixed 16 MiB array
+ * (4 Mi floats) in the library's device image, held by every GPU that loads
+ * the library until the process exits.  It runs passes of 16 right-hand
+ * sides, and a pass must fit in the array:
+ *   FP32 form:  16 floats per factor column (sum of ranks over both
+ *               orientations, padded to 8 per block), plus the chunk partials
+ *               of blocks with more than 1024 rows of V;
+ *   mixed form: 16 floats per point (X split into BF16 hi + lo fragments,
+ *               rows padded to 32 per leaf), plus 128 floats per
+ *               (row chunk, 8-column tile) of panels projected in several
+ *               row chunks, plus the projections (64 words per 8 factor
+ *               columns, 128 for columns with a low part).
+ * The 16 floats per point put the mixed form's limit near 2^18 points
+ * whatever the ranks.  A matrix beyond the array is rejected with
+ * HM_ERR_UNSUPPORTED and a message naming its need.
  *
  * The first call on a device resolves the array's device address on that
  * device (cudaGetSymbolAddress), so make that first call before any stream
- * capture.  All calls on a device share the one array and clear the part
- * they use before the product: calls whose work overlaps on the GPU (other
- * streams, other host threads) race and must be serialised by the caller. */
+ * capture.  All calls on a device share the one array, which keeps the last
+ * call's contents; every word of it that a product reads is written earlier
+ * in the same pass, so nothing needs clearing.  Calls whose work overlaps on
+ * the GPU (other streams, other host threads) race and must be serialised by
+ * the caller. */
 HM_API hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, int ldx, float* Y, int ldy,
                                     void* stream);
 
@@ -226,9 +291,11 @@ HM_API hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, int 
  * solver; it is the natural consumer of the product (hm_hmatvec).
  *
  * One CG per column, all columns sharing every product; X starts at zero.
- * Vectors are FP32, dot products FP64 in a fixed order.  The stream's work
- * is checked every `check_every` iterations: a column is done when
- * ||r|| <= tol ||b||, the solve when every column is.  On a created stream
+ * Vectors are FP32, dot products FP64 in a fixed order.  A column is done when
+ * ||r|| <= tol ||b|| on CG's recurrence; from then on it is frozen on the
+ * device (its X and r no longer change) while the other columns go on.  The
+ * host checks the stream's work every `check_every` iterations and stops when
+ * every column is done.  On a created stream
  * each chunk of check_every iterations is recorded once into a CUDA graph and
  * relaunched; on the legacy stream the iterations are launched directly.
  * Allocates its workspace (4 n x nrhs floats) from the stream-ordered pool
@@ -240,7 +307,7 @@ HM_API hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, int 
  * near that however small tol is.  Returns
  * HM_ERR_NOT_CONVERGED when max_iter iterations do not meet tol (X holds the
  * last iterate), HM_ERR_UNSUPPORTED when the operator shows itself not
- * positive definite (p.Ap <= 0). */
+ * positive definite (p.Ap <= 0 on a column that is not done). */
 HM_API hm_status hm_cg_solve(hm_hmatrix h, int nrhs, const float* B, int ldb, float* X, int ldx, double tol,
                              int max_iter, int check_every, void* stream, int* iterations, double* rel_residual);
 

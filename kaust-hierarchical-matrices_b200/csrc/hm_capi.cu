@@ -130,6 +130,23 @@ hm_status hm_kdtree_build(const double* d_points, int n, int d, int bucket, void
   return hm::kdtree_build(d_points, n, d, bucket, hm::as_stream(stream), out);
 }
 
+// The reference's division methods (src/kDTreeConstruction.cu:14-231):
+// DIVIDE_IN_HALF takes the same code path as FULL_TREE; POWER_OF_TWO_ON_LEFT
+// starts from upperPowerOfTwo(N) (:77-82) and halves that size per level, which
+// equals the ceil(len/2) split at every level exactly when N is a power of two.
+hm_status hm_kdtree_build_div(const double* d_points, int n, int d, int bucket, int division, void* stream,
+                              hm_kdtree* out) {
+  if (out) *out = nullptr;
+  if (division != HM_DIV_POWER_OF_TWO_ON_LEFT && division != HM_DIV_DIVIDE_IN_HALF &&
+      division != HM_DIV_FULL_TREE)
+    return hm::fail(HM_ERR_INVALID, "hm_kdtree_build_div: unknown division method " + std::to_string(division));
+  if (division == HM_DIV_POWER_OF_TWO_ON_LEFT && n > 0 && (n & (n - 1)) != 0)
+    return hm::fail(HM_ERR_UNSUPPORTED,
+                    "hm_kdtree_build_div: POWER_OF_TWO_ON_LEFT is supported for a power-of-two n only (where it "
+                    "equals FULL_TREE); n = " + std::to_string(n));
+  return hm::kdtree_build(d_points, n, d, bucket, hm::as_stream(stream), out);
+}
+
 hm_status hm_kdtree_info(hm_kdtree t, int* n, int* d, int* bucket, int* depth) {
   if (!t) return hm::fail(HM_ERR_INVALID, "hm_kdtree_info: null tree");
   if (n) *n = t->n;

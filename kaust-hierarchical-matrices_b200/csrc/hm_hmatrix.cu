@@ -1125,12 +1125,18 @@ size_t orth_smem() {
 
 }  // namespace
 
+// leaf_lo, leaf_hi: the block-row shard, leaves [leaf_lo, leaf_hi) (all
+// leaves for a whole matrix).  A shard compresses only the pairs whose row or
+// column cluster overlaps its rows, and only its own diagonal leaves.
 hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, const hm_build_opts* o,
-                        cudaStream_t stream, hm_hmatrix* out) {
+                        cudaStream_t stream, hm_hmatrix* out, int leaf_lo, int leaf_hi) {
   if (!out) return fail(HM_ERR_INVALID, "hm_hmatrix_build: out is NULL");
   *out = nullptr;
   if (!t || !s || !o) return fail(HM_ERR_INVALID, "hm_hmatrix_build: null argument");
   if (s->tree != t) return fail(HM_ERR_INVALID, "hm_hmatrix_build: structure was built on another tree");
+  if (leaf_hi < 0) leaf_hi = 1 << t->depth;
+  if (leaf_lo < 0 || leaf_lo >= leaf_hi || leaf_hi > (1 << t->depth))
+    return fail(HM_ERR_INVALID, "hm_hmatrix_build_rows: need 0 <= leaf_begin < leaf_end <= 2^depth");
   (void)d_points;  // the tree keeps its own tree-ordered copy of the points
   hm_build_opts opt = *o;
   if (opt.kernel < 0 || opt.kernel > 2) return fail(HM_ERR_INVALID, "hm_hmatrix_build: unknown kernel");
@@ -1162,6 +1168,8 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   h->d = t->d;
   h->depth = t->depth;
   h->opts = opt;
+  h->leaf_lo = leaf_lo;
+  h->leaf_hi = leaf_hi;
   h->kp.kind = opt.kernel;
   h->kp.deriv = opt.derivative ? 1 : 0;
   h->kp.ell = (float)opt.ell;
@@ -1170,6 +1178,11 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   const int depth = t->depth;
   const std::vector<int>& lo = t->h_offsets;
   auto coff = [&](int level, int c) { return lo[(size_t)c << (depth - level)]; };
+  // rows of the shard; a pair is needed when its rows or its columns overlap them
+  const int row_lo = lo[leaf_lo], row_hi = lo[leaf_hi];
+  auto needed = [&](int r0, int m, int c0, int n) {
+    return (r0 < row_hi && r0 + m > row_lo) || (c0 < row_hi && c0 + n > row_lo);
+  };
 
   PhaseTrace tr("build");
   // ---- the problems: stored pairs (row cluster v > column cluster u) ------
@@ -1191,27 +1204,41 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       P.c0 = coff(l, u);
       P.n = coff(l, u + 1) - P.c0;
       P.kmax = std::min(l == depth ? opt.leaf_max_rank : opt.max_rank, std::min(P.m, P.n));
+      if (!needed(P.r0, P.m, P.c0, P.n)) continue;
       probs.push_back(P);
     }
   }
-  const long long nprob = (long long)probs.size();
+  const long long nprob0 = (long long)probs.size();
 
   tr.mark("problems", stream);
   // ---- batches bounded by the workspace budget -----------------------------
   size_t freeb = 0, totb = 0;
   HM_CUDA(cudaMemGetInfo(&freeb, &totb));
   const size_t budget_bytes = std::min<size_t>(freeb / 4, (size_t)24 << 30);
-  std::vector<int> rank(nprob, 0), conv(nprob, 0), rhis(nprob, 0);
-  std::vector<double> nrm(nprob, 0.0);
+  // per-problem results that survive the batch: rank (-1: stored dense, -2:
+  // split into its child blocks), low-part columns, and the factor location.
+  // A problem that misses the tolerance at its rank cap above the leaf level
+  // appends its four child pairs to `probs`, so these grow with it.
+  std::vector<int> rank(nprob0, 0), conv(nprob0, 0), rhis(nprob0, 0);
+  std::vector<double> nrm(nprob0, 0.0);
   long long pstart = 0;
   const double thresh2 = 0.09 * opt.tol * opt.tol;  // (0.3 tol)^2
-  long long lr_count = 0, dense_count = 0, rank_sum = 0;
+  long long lr_count = 0, dense_count = 0, rank_sum = 0, split_count = 0;
   int max_rank_seen = 0;
   long long factor_bytes = 0, dense_bytes = 0, unconverged = 0;
 
-  // per-problem results that survive the batch: the factor location
-  std::vector<const float*> fu(nprob, nullptr), fv(nprob, nullptr);
-  std::vector<const float*> fd(nprob, nullptr), fdt(nprob, nullptr);
+  std::vector<const float*> fu(nprob0, nullptr), fv(nprob0, nullptr);
+  std::vector<const float*> fd(nprob0, nullptr), fdt(nprob0, nullptr);
+  auto grow = [&](size_t np) {
+    rank.resize(np, 0);
+    conv.resize(np, 0);
+    rhis.resize(np, 0);
+    nrm.resize(np, 0.0);
+    fu.resize(np, nullptr);
+    fv.resize(np, nullptr);
+    fd.resize(np, nullptr);
+    fdt.resize(np, nullptr);
+  };
 
   // Sketches, bases and projections run in FP64 when the tolerance is below
   // what FP32 sums over a block can resolve (~u*sqrt(m) relative), else FP32.
@@ -1232,31 +1259,40 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
     const int bst = 0;
     const int bs_first = fastW ? std::min(2 * bs, kMaxBs) : bs;  // round 0 basis columns
     const int wmax = std::max(bs_first, bs) + bst;                // widest sample
-    // greedy batches under the workspace budget; one workspace for all of them
-    std::vector<long long> batch_end;
-    size_t ws_max = 1;
-    for (long long ps = pstart; ps < nprob;) {
+    // greedy batches under the workspace budget; one workspace for all of
+    // them (child blocks of split problems come in later batches, whose
+    // workspace is no larger unless a batch of them packs tighter)
+    auto next_batch = [&](long long ps, size_t* wsz_out) {
       long long pe = ps;
       size_t wsz = 0;
-      while (pe < nprob) {
+      while (pe < (long long)probs.size()) {
         const Prob& P = probs[pe];
         size_t need = (size_t)P.m * (P.kmax + wmax) + (size_t)P.m * wmax + (size_t)P.n * (P.kmax + wmax);
         if (pe > ps && wsz + need > budget_elems) break;
         wsz += need;
         ++pe;
       }
-      batch_end.push_back(pe);
-      ws_max = std::max(ws_max, wsz);
-      ps = pe;
+      *wsz_out = wsz;
+      return pe;
+    };
+    size_t ws_max = 1;
+    for (long long ps = pstart; ps < (long long)probs.size();) {
+      size_t w = 0;
+      ps = next_batch(ps, &w);
+      ws_max = std::max(ws_max, w);
     }
     DevBuf<W> ws;
     {
       hm_status st0 = ws.alloc(ws_max);
       if (st0) return st0;
     }
-    size_t bi = 0;
-    while (pstart < nprob) {
-      const long long pend = batch_end[bi++];
+    while (pstart < (long long)probs.size()) {
+      size_t wsz = 0;
+      const long long pend = next_batch(pstart, &wsz);
+      if (wsz > ws.n) {
+        hm_status st0 = ws.alloc(wsz);
+        if (st0) return st0;
+      }
       const int nb = (int)(pend - pstart);
       tr.mark("batch begin", stream, nb);
       std::vector<Prob> bp(probs.begin() + pstart, probs.begin() + pend);
@@ -1478,23 +1514,43 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       HM_CUDA(cudaStreamSynchronize(stream));
 
       tr.mark("truncation", stream, nb);
-      // ---- results: low rank where converged, dense otherwise ---------------
+      // ---- results: low rank where converged; otherwise the four child
+      // blocks (above the leaf level) or dense (leaf blocks) -----------------
       std::vector<long long> du(nb, -1), dv(nb, -1);
       std::vector<DenseItem> dens;
+      std::vector<Prob> children;
       size_t chunk_floats = 0;
       for (int i = 0; i < nb; ++i) {
         const Prob& P = bp[i];
         const ProbState& S = hst[i];
         long long gi = pstart + i;
         nrm[gi] = S.normA2;
-        // a block that missed the tolerance at its rank cap is stored dense when
-        // that is affordable (leaf blocks always are; others up to 2^22
-        // entries); a larger one keeps its capped factors and is counted as
-        // unconverged
-        const bool small = (size_t)P.m * P.n <=
-                           std::max((size_t)1 << 22, 2 * (size_t)(P.m + P.n) * (size_t)std::max(S.k, 1));
-        if (!(S.converged || S.active) && !(P.level == depth || small)) ++unconverged;
-        if (S.converged || S.active || !(P.level == depth || small)) {
+        const bool capped = !(S.converged || S.active);
+        if (capped && P.level < depth) {
+          // the pair as the reference's recursion would have recorded it had
+          // it been inadmissible (src/HMatrixStructure.cu:27-89): its four
+          // child pairs (2v + b, 2u + a), compressed in a later batch; every
+          // child keeps row cluster > column cluster
+          rank[gi] = -2;
+          ++split_count;
+          const int cl = P.level + 1;
+          for (int b2 = 0; b2 < 2; ++b2)
+            for (int a2 = 0; a2 < 2; ++a2) {
+              Prob C{};
+              C.level = cl;
+              C.u = 2 * P.u + a2;
+              C.v = 2 * P.v + b2;
+              C.r0 = coff(cl, C.v);
+              C.m = coff(cl, C.v + 1) - C.r0;
+              C.c0 = coff(cl, C.u);
+              C.n = coff(cl, C.u + 1) - C.c0;
+              if (C.m <= 0 || C.n <= 0 || !needed(C.r0, C.m, C.c0, C.n)) continue;
+              C.kmax = std::min(cl == depth ? opt.leaf_max_rank : opt.max_rank, std::min(C.m, C.n));
+              children.push_back(C);
+            }
+          continue;
+        }
+        if (!capped) {
           du[i] = (long long)chunk_floats;
           chunk_floats += (size_t)P.m * S.r;
           dv[i] = (long long)chunk_floats;
@@ -1545,6 +1601,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       size_t pk = 0, dk = 0;
       for (int i = 0; i < nb; ++i) {
         long long gi = pstart + i;
+        if (rank[gi] == -2) continue;  // split
         if (rank[gi] >= 0) {
           fu[gi] = chunk.p + du[i];
           fv[gi] = chunk.p + dv[i];
@@ -1564,6 +1621,11 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       tr.mark("factors", stream, nb);
       h->storage.push_back(std::move(chunk));
       pstart = pend;
+      if (!children.empty()) {
+        probs.insert(probs.end(), children.begin(), children.end());
+        grow(probs.size());
+        tr.mark("split into children", stream, (long long)children.size());
+      }
     }
     return HM_OK;
   };
@@ -1573,28 +1635,29 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   }
 
   // ---- diagonal leaves ------------------------------------------------------
-  const int nleaf = 1 << depth;
   h->diag_fly = opt.diag_from_coords > 0 || (opt.diag_from_coords < 0 && opt.derivative != 0);
   if (!h->diag_fly) {
-    std::vector<DenseItem> dens(nleaf);
+    const int nown = leaf_hi - leaf_lo;  // the shard's leaves (all of them for a whole matrix)
+    std::vector<DenseItem> dens(nown);
     size_t tot = 0;
-    for (int l = 0; l < nleaf; ++l) {
-      dens[l].r0 = lo[l];
-      dens[l].m = lo[l + 1] - lo[l];
-      dens[l].c0 = lo[l];
-      dens[l].n = dens[l].m;
-      dens[l].off = (long long)tot;
-      tot += (size_t)dens[l].m * dens[l].m;
+    for (int q = 0; q < nown; ++q) {
+      const int l = leaf_lo + q;
+      dens[q].r0 = lo[l];
+      dens[q].m = lo[l + 1] - lo[l];
+      dens[q].c0 = lo[l];
+      dens[q].n = dens[q].m;
+      dens[q].off = (long long)tot;
+      tot += (size_t)dens[q].m * dens[q].m;
     }
     DevBuf<float> chunk;
     DevBuf<DenseItem> ddi;
     hm_status st;
-    if ((st = chunk.alloc(std::max<size_t>(tot, 1))) || (st = ddi.alloc(nleaf))) return cleanup(st);
-    HM_CUDA(cudaMemcpyAsync(ddi.p, dens.data(), sizeof(DenseItem) * nleaf, cudaMemcpyHostToDevice, stream));
-    k_dense_gen<<<nleaf, 256, 0, stream>>>(ddi.p, t->pts_tree_f.p, t->n, t->d, h->kp, chunk.p);
+    if ((st = chunk.alloc(std::max<size_t>(tot, 1))) || (st = ddi.alloc(nown))) return cleanup(st);
+    HM_CUDA(cudaMemcpyAsync(ddi.p, dens.data(), sizeof(DenseItem) * nown, cudaMemcpyHostToDevice, stream));
+    k_dense_gen<<<nown, 256, 0, stream>>>(ddi.p, t->pts_tree_f.p, t->n, t->d, h->kp, chunk.p);
     HM_LAUNCH_CHECK();
     HM_CUDA(cudaStreamSynchronize(stream));
-    for (int l = 0; l < nleaf; ++l) {
+    for (int l = 0; l < nown; ++l) {
       DenseBlock db;
       db.r0 = dens[l].r0;
       db.m = dens[l].m;
@@ -1604,15 +1667,17 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       db.D = chunk.p + dens[l].off;
       if (db.m > 0) h->h_dense.push_back(db);
     }
-    dense_count += nleaf;
+    dense_count += nown;
     dense_bytes += 4ll * (long long)tot;
     h->storage.push_back(std::move(chunk));
   }
 
   tr.mark("diagonal leaves", stream);
   // ---- block lists (both orientations) --------------------------------------
+  const long long nprob = (long long)probs.size();
   for (long long i = 0; i < nprob; ++i) {
     const Prob& P = probs[i];
+    if (rank[i] == -2) continue;  // split: its children are in the list
     if (rank[i] >= 0) {
       LRBlock b{};
       b.level = P.level;
@@ -1662,6 +1727,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   h->stats.factor_bytes = factor_bytes;
   h->stats.dense_bytes = dense_bytes;
   h->stats.num_unconverged = unconverged;
+  h->stats.num_split = split_count;
   tr.mark("mixed panels", stream);
   hm_status st = matvec_plan_build(h, 16, stream);
   if (st) return cleanup(st);
@@ -1675,6 +1741,21 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   cudaEventDestroy(ev1);
   *out = h;
   return HM_OK;
+}
+
+// Device memory held by the matrix: factor and dense storage, the mixed
+// form's panels and tables, the product's plan and workspaces.
+long long device_bytes(const hm_hmatrix_s* h) {
+  long long b = 0;
+  auto add = [&b](const auto& buf) { b += (long long)(buf.n * sizeof(*buf.p)); };
+  for (const auto& c : h->storage) add(c);
+  const MatvecPlan& P = h->plan;
+  add(P.lr), add(P.p1), add(P.multi), add(P.groups), add(P.leaf_ptr), add(P.leaf_blk), add(P.dense);
+  add(P.leaf_dptr), add(P.leaf_dblk), add(P.T), add(P.Xp), add(P.Yp);
+  const MxPlan& M = h->mx;
+  add(M.store), add(M.panels), add(M.pan_of), add(M.units), add(M.tile_leaf), add(M.leaf_tile0), add(M.tslot);
+  add(M.mtiles), add(M.dense), add(M.leaf_dptr), add(M.leaf_dblk);
+  return b;
 }
 
 }  // namespace hm
@@ -1698,12 +1779,22 @@ void hm_build_opts_default(int d, hm_build_opts* o) {
 
 hm_status hm_hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, const hm_build_opts* opts,
                            void* stream, hm_hmatrix* out) {
-  return hm::hmatrix_build(t, s, d_points, opts, hm::as_stream(stream), out);
+  return hm::hmatrix_build(t, s, d_points, opts, hm::as_stream(stream), out, 0, -1);
+}
+
+hm_status hm_hmatrix_build_rows(hm_kdtree t, hm_structure s, const double* d_points, const hm_build_opts* opts,
+                                int leaf_begin, int leaf_end, void* stream, hm_hmatrix* out) {
+  if (out) *out = nullptr;
+  if (!t) return hm::fail(HM_ERR_INVALID, "hm_hmatrix_build_rows: null tree");
+  if (leaf_begin < 0 || leaf_begin >= leaf_end || leaf_end > (1 << t->depth))
+    return hm::fail(HM_ERR_INVALID, "hm_hmatrix_build_rows: need 0 <= leaf_begin < leaf_end <= 2^depth");
+  return hm::hmatrix_build(t, s, d_points, opts, hm::as_stream(stream), out, leaf_begin, leaf_end);
 }
 
 hm_status hm_hmatrix_stats_get(hm_hmatrix h, hm_hmatrix_stats* st) {
   if (!h || !st) return hm::fail(HM_ERR_INVALID, "hm_hmatrix_stats_get: null argument");
   *st = h->stats;
+  st->device_bytes = hm::device_bytes(h);
   return HM_OK;
 }
 

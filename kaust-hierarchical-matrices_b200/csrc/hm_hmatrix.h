@@ -87,6 +87,11 @@ struct MatvecPlan {
 
 }  // namespace hm
 
+struct hm_hmatrix_s;
+namespace hm {
+long long device_bytes(const hm_hmatrix_s* h);
+}  // namespace hm
+
 struct hm_hmatrix_s {
   hm_kdtree tree = nullptr;        // not owned
   hm_structure structure = nullptr;  // not owned
@@ -98,6 +103,7 @@ struct hm_hmatrix_s {
   hm::MatvecPlan plan;
   hm::MxPlan mx;                     // mixed precision form (panels of BF16 hi + lo tiles)
   bool diag_fly = false;             // diagonal leaf blocks recomputed from the coordinates per product
+  int leaf_lo = 0, leaf_hi = 0;      // block-row shard: the product's rows are those of leaves [leaf_lo, leaf_hi)
   int plan_gen = 0;                  // bumped whenever the product's plan is rebuilt
   // host mirror of the block list (for export / tests)
   std::vector<hm::LRBlock> h_lr;

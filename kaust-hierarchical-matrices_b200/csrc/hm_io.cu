@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <new>
 #include <vector>
 
 #include "hm_hmatrix.h"
@@ -92,6 +93,9 @@ struct DenseRec {
 extern "C" hm_status hm_hmatrix_save(hm_hmatrix h, const char* path) {
   using namespace hm;
   if (!h || !path) return fail(HM_ERR_INVALID, "hm_hmatrix_save: null argument");
+  if (h->leaf_lo != 0 || h->leaf_hi != (1 << h->depth))
+    return fail(HM_ERR_UNSUPPORTED, "hm_hmatrix_save: a block-row shard is saved as part of no file format; save "
+                                    "the whole matrix");
   // every stored pair sits in h_lr as (block, mirror) at 2i, 2i + 1
   if (h->h_lr.size() % 2) return fail(HM_ERR_UNSUPPORTED, "hm_hmatrix_save: unpaired block list");
   auto locate = [&](const float* p, int32_t* c, int64_t* o) {
@@ -168,22 +172,35 @@ extern "C" hm_status hm_hmatrix_save(hm_hmatrix h, const char* path) {
   return HM_OK;
 }
 
-extern "C" hm_status hm_hmatrix_load(hm_kdtree t, hm_structure s, const char* path, void* stream,
-                                     hm_hmatrix* result) {
-  using namespace hm;
-  if (!result) return fail(HM_ERR_INVALID, "hm_hmatrix_load: out is NULL");
-  *result = nullptr;
+namespace hm {
+namespace {
+
+// The body of hm_hmatrix_load.  Every count read from the file is checked
+// against the bytes the file has left before anything is sized by it, and
+// every block's extent is checked in 64-bit arithmetic, so a damaged or
+// foreign file is refused with HM_ERR_INVALID.
+hm_status load_impl(hm_kdtree t, hm_structure s, const char* path, void* stream, hm_hmatrix* result) {
   if (!t || !s || !path) return fail(HM_ERR_INVALID, "hm_hmatrix_load: null argument");
   if (s->tree != t) return fail(HM_ERR_INVALID, "hm_hmatrix_load: structure was built on another tree");
   cudaStream_t st = as_stream(stream);
   File in;
   in.f = std::fopen(path, "rb");
   if (!in.f) return fail(HM_ERR_INVALID, std::string("hm_hmatrix_load: cannot open ") + path);
+  long long fsize = -1;
+  if (std::fseek(in.f, 0, SEEK_END) == 0) fsize = std::ftell(in.f);
+  if (fsize < 0 || std::fseek(in.f, 0, SEEK_SET) != 0)
+    return fail(HM_ERR_INVALID, std::string("hm_hmatrix_load: cannot size ") + path);
+  long long pos = 0;
   bool ok = true;
   auto get = [&](void* p, size_t bytes) {
-    if (ok && bytes) ok = std::fread(p, 1, bytes, in.f) == bytes;
+    if (ok && bytes) {
+      ok = std::fread(p, 1, bytes, in.f) == bytes;
+      pos += (long long)bytes;
+    }
     return ok;
   };
+  // at most `count` records of `size` bytes fit in what is left of the file
+  auto fits = [&](long long count, size_t size) { return count >= 0 && count <= (fsize - pos) / (long long)size; };
   auto bad = [&](const std::string& why) { return fail(HM_ERR_INVALID, "hm_hmatrix_load: " + why + ": " + path); };
   char magic[8];
   uint32_t vers[3];
@@ -202,27 +219,36 @@ extern "C" hm_status hm_hmatrix_load(hm_kdtree t, hm_structure s, const char* pa
   HM_TRY(fingerprint(t, s, &mine));
   if (mine != fp) return bad("the tree or structure differs from the one the matrix was built on");
   int64_t nch = 0;
-  if (!get(&nch, sizeof nch) || nch < 0 || nch > (1 << 20)) return bad("bad chunk count");
+  if (!get(&nch, sizeof nch) || nch < 0 || nch > (1 << 20) || !fits(nch, sizeof(uint64_t)))
+    return bad("bad chunk count");
   std::vector<uint64_t> nf((size_t)nch);
   if (!get(nf.data(), sizeof(uint64_t) * nf.size())) return bad("truncated chunk table");
   int64_t np = 0, nd = 0;
-  if (!get(&np, sizeof np) || np < 0 || np > (1ll << 40)) return bad("bad pair count");
+  if (!get(&np, sizeof np) || !fits(np, sizeof(PairRec))) return bad("bad pair count");
   std::vector<PairRec> pairs((size_t)np);
-  if (!get(pairs.data(), sizeof(PairRec) * pairs.size()) || !get(&nd, sizeof nd) || nd < 0 || nd > (1ll << 40))
+  if (!get(pairs.data(), sizeof(PairRec) * pairs.size()) || !get(&nd, sizeof nd) || !fits(nd, sizeof(DenseRec)))
     return bad("truncated pair list");
   std::vector<DenseRec> dense((size_t)nd);
   if (!get(dense.data(), sizeof(DenseRec) * dense.size())) return bad("truncated dense list");
+  // the factor data: what the chunk table claims must be what the file holds
+  long long data_floats = 0;
+  for (uint64_t c : nf) {
+    if (c > (uint64_t)(fsize / 4)) return bad("bad chunk size");
+    data_floats += (long long)c;
+  }
+  if (data_floats != (fsize - pos) / 4 || (fsize - pos) % 4 != 0) return bad("factor data of the wrong length");
   // every reference must lie inside its chunk
   auto inside = [&](int32_t c, int64_t o, long long len) {
-    return c >= 0 && c < nch && o >= 0 && len >= 0 && (uint64_t)(o + len) <= nf[c];
+    return c >= 0 && c < nch && o >= 0 && len >= 0 && (uint64_t)o + (uint64_t)len <= nf[c];
   };
+  const long long n64 = t->n;
   for (const PairRec& r : pairs)
-    if (r.m <= 0 || r.n <= 0 || r.k <= 0 || r.khi < 0 || r.khi > r.k || r.r0 < 0 || r.c0 < 0 ||
-        r.r0 + r.m > t->n || r.c0 + r.n > t->n || !inside(r.cu, r.ou, (long long)r.m * r.k) ||
-        !inside(r.cv, r.ov, (long long)r.n * r.k))
+    if (r.m <= 0 || r.n <= 0 || r.k <= 0 || r.k > 256 || r.khi < 0 || r.khi > r.k || r.level < 1 ||
+        r.level > t->depth || r.r0 < 0 || r.c0 < 0 || (long long)r.r0 + r.m > n64 || (long long)r.c0 + r.n > n64 ||
+        !inside(r.cu, r.ou, (long long)r.m * r.k) || !inside(r.cv, r.ov, (long long)r.n * r.k))
       return bad("a low-rank pair outside the matrix or its data");
   for (const DenseRec& r : dense)
-    if (r.m < 0 || r.n < 0 || r.r0 < 0 || r.c0 < 0 || r.r0 + r.m > t->n || r.c0 + r.n > t->n ||
+    if (r.m < 0 || r.n < 0 || r.r0 < 0 || r.c0 < 0 || (long long)r.r0 + r.m > n64 || (long long)r.c0 + r.n > n64 ||
         !inside(r.c, r.o, (long long)r.m * r.n))
       return bad("a dense block outside the matrix or its data");
 
@@ -231,6 +257,8 @@ extern "C" hm_status hm_hmatrix_load(hm_kdtree t, hm_structure s, const char* pa
   h->n = t->n;
   h->d = t->d;
   h->depth = t->depth;
+  h->leaf_lo = 0;
+  h->leaf_hi = 1 << t->depth;
   h->diag_fly = dims[3] != 0;
   h->kp.kind = h->opts.kernel;
   h->kp.deriv = h->opts.derivative ? 1 : 0;
@@ -282,4 +310,18 @@ extern "C" hm_status hm_hmatrix_load(hm_kdtree t, hm_structure s, const char* pa
   HM_CUDA(cudaStreamSynchronize(st));
   *result = h.release();
   return HM_OK;
+}
+
+}  // namespace
+}  // namespace hm
+
+extern "C" hm_status hm_hmatrix_load(hm_kdtree t, hm_structure s, const char* path, void* stream,
+                                     hm_hmatrix* result) {
+  if (!result) return hm::fail(HM_ERR_INVALID, "hm_hmatrix_load: out is NULL");
+  *result = nullptr;
+  try {
+    return hm::load_impl(t, s, path, stream, result);
+  } catch (const std::bad_alloc&) {
+    return hm::fail(HM_ERR_NOMEM, "hm_hmatrix_load: out of host memory");
+  }
 }

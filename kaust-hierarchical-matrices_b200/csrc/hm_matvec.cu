@@ -276,6 +276,30 @@ __global__ void k_scatter_rows(const float* Yp, const int* perm, int n, int nrhs
 }
 
 
+// FP64 vectors of the reference's interface: X (double, ldx; rows gathered
+// through perm when perm != null) narrowed into Xp (float, ld n) ...
+__global__ void k_narrow_rows(const double* __restrict__ X, int ldx, const int* __restrict__ perm, int n, int nrhs,
+                              float* __restrict__ Xp) {
+  long long tot = (long long)n * nrhs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(e % n), c = (int)(e / n);
+    Xp[(size_t)c * n + i] = (float)X[(size_t)c * ldx + (perm ? perm[i] : i)];
+  }
+}
+
+// ... and the FP32 result Yp (ld n) widened into Y (double, ldy; rows
+// scattered through perm when perm != null)
+__global__ void k_widen_rows(const float* __restrict__ Yp, const int* __restrict__ perm, int n, int nrhs,
+                             double* __restrict__ Y, int ldy) {
+  long long tot = (long long)n * nrhs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(e % n), c = (int)(e / n);
+    Y[(size_t)c * ldy + (perm ? perm[i] : i)] = (double)Yp[(size_t)c * n + i];
+  }
+}
+
 // Y[leaf] += K(leaf, leaf) X[leaf], one CTA per leaf, entries from the
 // tree-ordered FP32 coordinates exactly as the stored diagonal blocks are
 // generated (kernel_r2, plus the nugget on the diagonal unless dK/dl).
@@ -370,7 +394,11 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   // 128 columns (U and V sliced alike), whose products add up
   std::vector<LRBlock> lr;
   lr.reserve(h->h_lr.size());
+  // a block-row shard expands only into its own rows [row_lo, row_hi)
+  const int row_lo = lo[h->leaf_lo], row_hi = lo[h->leaf_hi];
+  auto own_rows = [&](int r0, int m) { return r0 < row_hi && r0 + m > row_lo; };
   for (const LRBlock& b : h->h_lr) {
+    if (!own_rows(b.r0, b.m)) continue;
     for (int c0 = 0; c0 == 0 || c0 < b.k; c0 += kMaxK) {
       LRBlock x = b;
       x.k = std::min(kMaxK, b.k - c0);
@@ -411,7 +439,8 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
     P.bytes_p1 += 4ll * b.n * b.k;
     P.bytes_p2 += 4ll * b.m * b.k;
   }
-  for (const auto& d : h->h_dense) P.bytes_p2 += 4ll * d.m * d.n;
+  for (const auto& d : h->h_dense)
+    if (own_rows(d.r0, d.m)) P.bytes_p2 += 4ll * d.m * d.n;
   for (const auto& mi : multi) P.multi_t_floats += 16ll * mi.kpad;
   // phase 2: leaf lists
   auto leaf_range = [&](int r0, int m, int& a, int& b) {
@@ -430,6 +459,8 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   for (size_t i = 0; i < h->h_dense.size(); ++i) {
     int a, e;
     leaf_range(h->h_dense[i].r0, h->h_dense[i].m, a, e);
+    a = std::max(a, h->leaf_lo);
+    e = std::max(a, std::min(e, h->leaf_hi));
     dranges[i] = {a, e};
     for (int l = a; l < e; ++l) dcnt[l]++;
   }
@@ -447,7 +478,7 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   for (size_t i = 0; i < h->h_dense.size(); ++i)
     for (int l = dranges[i].first; l < dranges[i].second; ++l) dblk[dfill[l]++] = (int)i;
   std::vector<int2> groups;
-  for (int l = 0; l < nleaf; ++l)
+  for (int l = h->leaf_lo; l < h->leaf_hi; ++l)
     for (int r = 0; r < lo[l + 1] - lo[l]; r += 32) groups.push_back(make_int2(l, r));
   P.num_groups = (int)groups.size();
 
@@ -519,6 +550,31 @@ hm_status hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, int ldx, fl
   return HM_OK;
 }
 
+// The product on FP64 vectors: per pass, X narrowed into the plan's Xp, the
+// FP32 product into Yp, Yp widened into Y; the permutation of original-order
+// calls is applied by the same two kernels.
+hm_status hmatvec_f64(hm_hmatrix h, int trans, int nrhs, const double* X, int ldx, double* Y, int ldy,
+                      int original_order, cudaStream_t stream) {
+  if (!h) return fail(HM_ERR_INVALID, "hm_hmatvec_f64: null matrix");
+  if (nrhs < 1 || !X || !Y || ldx < h->n || ldy < h->n)
+    return fail(HM_ERR_INVALID, "hm_hmatvec_f64: bad vector arguments");
+  if (trans != 0 && trans != 1) return fail(HM_ERR_INVALID, "hm_hmatvec_f64: trans must be 0 or 1");
+  // H^T X = H X: the stored operator is exactly symmetric (see hmatvec)
+  MatvecPlan& P = h->plan;
+  const int n = h->n;
+  const int* perm = original_order ? h->tree->perm.p : nullptr;
+  for (int c0 = 0; c0 < nrhs;) {
+    const int nr = std::min(pass_width(h), nrhs - c0);
+    k_narrow_rows<<<592, 256, 0, stream>>>(X + (size_t)c0 * ldx, ldx, perm, n, nr, P.Xp.p);
+    HM_LAUNCH_CHECK();
+    HM_TRY(run_panel(h, nr, P.Xp.p, n, P.Yp.p, n, P.T.p, stream, nullptr));
+    k_widen_rows<<<592, 256, 0, stream>>>(P.Yp.p, perm, n, nr, Y + (size_t)c0 * ldy, ldy);
+    HM_LAUNCH_CHECK();
+    c0 += nr;
+  }
+  return HM_OK;
+}
+
 // Algorithmic bytes of one product with nrhs FP32 columns: factors and dense
 // blocks read once, X read once and Y written once per phase that touches them.
 void matvec_bytes(hm_hmatrix h, int nrhs, long long* b_project, long long* b_expand) {
@@ -571,9 +627,10 @@ hm_status noalloc_scratch(float** out) {
 namespace hm {
 hm_status diag_fly_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, cudaStream_t s,
                          KernelMarks* km) {
-  const int nleaf = 1 << h->depth;
   const hm_kdtree t = h->tree;
-  k_diag_fly<<<nleaf, kFlyT, 0, s>>>(t->offsets.p, t->pts_tree_f.p, t->n, t->d, h->kp, X, ldx, nr, Y, ldy);
+  // the shard's leaves (every leaf of a whole matrix)
+  k_diag_fly<<<h->leaf_hi - h->leaf_lo, kFlyT, 0, s>>>(t->offsets.p + h->leaf_lo, t->pts_tree_f.p, t->n, t->d,
+                                                       h->kp, X, ldx, nr, Y, ldy);
   HM_LAUNCH_CHECK();
   if (km) km->mark("k_diag_fly", 4ll * h->n * nr * 3 + 4ll * h->n * h->d, s);
   return HM_OK;
@@ -602,18 +659,24 @@ extern "C" hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, 
     return hm::fail(HM_ERR_INVALID, "hm_hmatvec_noalloc: bad vector arguments");
   hm::MatvecPlan& P = h->plan;
   const size_t need = h->mx.enabled ? (size_t)h->mx.scratch_floats() : (size_t)P.t_floats + (size_t)P.part_floats;
-  if (need > hm::kNoallocScratchFloats)
-    return hm::fail(HM_ERR_UNSUPPORTED,
-                    "hm_hmatvec_noalloc: this matrix needs " + std::to_string(need) +
-                        " floats of projection scratch (sum of ranks x 16, plus chunk partials); the static scratch holds " +
-                        std::to_string(hm::kNoallocScratchFloats) + " (16 MiB)");
+  if (need > hm::kNoallocScratchFloats) {
+    const std::string what =
+        h->mx.enabled ? " floats of scratch for a 16-column pass of the mixed form (16 per point for the X "
+                        "fragments, plus chunk partials and projections)"
+                      : " floats of projection scratch for a 16-column pass of the FP32 form (16 per factor "
+                        "column, plus chunk partials)";
+    return hm::fail(HM_ERR_UNSUPPORTED, "hm_hmatvec_noalloc: this matrix needs " + std::to_string(need) + what +
+                                            "; the static scratch holds " +
+                                            std::to_string(hm::kNoallocScratchFloats) + " (16 MiB)");
+  }
   float* T = nullptr;
   HM_TRY(hm::noalloc_scratch(&T));
   cudaStream_t s = hm::as_stream(stream);
   for (int c0 = 0; c0 < nrhs;) {
     const int nr = std::min(16, nrhs - c0);
-    // the scratch keeps the previous call's contents: the projections that are
-    // summed must start at zero (run_panel clears them, the others are stored)
+    // the scratch keeps the previous call's contents, which need no clearing:
+    // every scratch word the pass reads (X fragments, chunk partials,
+    // projections, padding columns as zeros) is written earlier in the pass
     HM_TRY(hm::run_panel(h, nr, X + (size_t)c0 * ldx, ldx, Y + (size_t)c0 * ldy, ldy, T, s, nullptr));
     c0 += nr;
   }
@@ -623,6 +686,11 @@ extern "C" hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, 
 extern "C" hm_status hm_hmatvec(hm_hmatrix h, int trans, int nrhs, const float* X, int ldx, float* Y, int ldy,
                                 int original_order, void* stream) {
   return hm::hmatvec(h, trans, nrhs, X, ldx, Y, ldy, original_order, hm::as_stream(stream));
+}
+
+extern "C" hm_status hm_hmatvec_f64(hm_hmatrix h, int trans, int nrhs, const double* X, int ldx, double* Y, int ldy,
+                                    int original_order, void* stream) {
+  return hm::hmatvec_f64(h, trans, nrhs, X, ldx, Y, ldy, original_order, hm::as_stream(stream));
 }
 
 extern "C" hm_status hm_hmatvec_profile(hm_hmatrix h, int nrhs, const float* X, int ldx, float* Y, int ldy,

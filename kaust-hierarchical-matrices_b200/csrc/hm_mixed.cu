@@ -481,15 +481,16 @@ __device__ __forceinline__ void mx_p2_step_hi(float (&acc)[2][2][4], const uint4
 constexpr int kP2Warps = 1, kP2PerSm = 28, kP2PerSm2 = 16;
 template <int NH>
 __global__ void __launch_bounds__(32 * kP2Warps, (NH == 1 ? kP2PerSm : kP2PerSm2) / kP2Warps)
-    k_mx_p2(int num_tiles, int depth, const int* __restrict__ tile_leaf,
+    k_mx_p2(int tile0, int tile_end, int depth, const int* __restrict__ tile_leaf,
                                                const int* __restrict__ leaf_tile0, const int* __restrict__ leaf_off,
                                                const int* __restrict__ pan_of, const MxPanel* __restrict__ panels,
                                                const uint4* __restrict__ store, const uint32_t* __restrict__ T,
                                                const int* __restrict__ leaf_dptr, const int* __restrict__ leaf_dblk,
                                                const MxDense* __restrict__ dense, const uint4* __restrict__ Xf,
                                                float* __restrict__ Y, int ldy, int nr, long long xh_, long long th) {
-  const int G = blockIdx.x * kP2Warps + (threadIdx.x >> 5);
-  if (G >= num_tiles) return;
+  // global row tiles [tile0, tile_end): every tile, or a block-row shard's
+  const int G = tile0 + blockIdx.x * kP2Warps + (threadIdx.x >> 5);
+  if (G >= tile_end) return;
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int x = tile_leaf[G];
   float acc[NH][2][2][4];
@@ -720,6 +721,9 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   }
   leaf_tile0[nleaf] = (int)tile_leaf.size();
   M.num_tiles = (int)tile_leaf.size();
+  // phase 2 runs over the row tiles of the matrix's rows (a block-row shard's own leaves)
+  M.p2_tile0 = leaf_tile0[h->leaf_lo];
+  M.p2_tiles = leaf_tile0[h->leaf_hi] - M.p2_tile0;
 
   // leaf range [first, end) of the cluster whose rows are [r0, r0 + m)
   auto leaf_range = [&](int r0, int m, int* first, int* end) {
@@ -1020,20 +1024,21 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_mx_reduce", (512ll * M.s_tiles + 512ll * M.nmt) * nh, s);
   }
-  if (M.num_tiles > 0) {
-    const unsigned grid = (unsigned)((M.num_tiles + kP2Warps - 1) / kP2Warps);
+  if (M.p2_tiles > 0) {
+    const unsigned grid = (unsigned)((M.p2_tiles + kP2Warps - 1) / kP2Warps);
+    const int te = M.p2_tile0 + M.p2_tiles;
     if (nh == 1)
-      k_mx_p2<1><<<grid, 32 * kP2Warps, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
+      k_mx_p2<1><<<grid, 32 * kP2Warps, 0, s>>>(M.p2_tile0, te, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
                                                 M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p, M.leaf_dblk.p,
                                                 M.dense.p, Xf, Y, ldy, nr, xh, th);
     else if (nh == 2)
-      k_mx_p2<2><<<grid, 32 * kP2Warps, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
+      k_mx_p2<2><<<grid, 32 * kP2Warps, 0, s>>>(M.p2_tile0, te, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
                                                 M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p, M.leaf_dblk.p,
                                                 M.dense.p, Xf, Y, ldy, nr, xh, th);
     else  // four parts: two launches of two parts each (a four-part phase 2 spills
           // at 128 registers and measured slower than two of these)
       for (int q = 0; q < 2 && nr > 32 * q; ++q)
-        k_mx_p2<2><<<grid, 32 * kP2Warps, 0, s>>>(M.num_tiles, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
+        k_mx_p2<2><<<grid, 32 * kP2Warps, 0, s>>>(M.p2_tile0, te, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
                                                   M.pan_of.p, M.panels.p, M.store.p, T + 2 * q * th, M.leaf_dptr.p,
                                                   M.leaf_dblk.p, M.dense.p, Xf + 2 * q * xh, Y + (size_t)32 * q * ldy,
                                                   ldy, std::min(32, nr - 32 * q), xh, th);

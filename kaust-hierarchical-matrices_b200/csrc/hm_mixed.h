@@ -66,6 +66,7 @@ struct MxPlan {
   DevBuf<int> tile_leaf;   // global row tile -> leaf
   DevBuf<int> leaf_tile0;  // leaf -> first global row tile (num_leaves + 1)
   int num_tiles = 0;
+  int p2_tile0 = 0, p2_tiles = 0;  // row tiles phase 2 writes (all, or a block-row shard's)
   // global factor column (8 * t0 + c) -> where its projection goes in T:
   // (word << 1) | h, word = the column's first 32-bit word at lane row 0 (row
   // g adds 16 g words in a tile with low parts, 8 g in one without), h = 1

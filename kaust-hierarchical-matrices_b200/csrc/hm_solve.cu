@@ -10,8 +10,9 @@
 // beta live on the device: a chunk of `check_every` iterations needs no host
 // synchronisation, and on a created stream it is recorded once into a CUDA
 // graph and relaunched.  Between chunks the host reads the residual norms
-// and stops when every column meets the tolerance.  A column whose residual
-// reaches zero (or whose right-hand side is zero) stops moving.
+// and stops when every column meets the tolerance.  A column that meets the
+// tolerance (a zero residual or right-hand side included) stops moving at
+// once, on the device, while the others go on.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -69,9 +70,12 @@ __global__ void __launch_bounds__(kCgThreads) k_cg_dot(const float* __restrict__
 
 // Per column, the sum of its partials, in block order.  which: 0 start
 // (bb = rr = sum), 1 alpha (sum = p.Ap), 2 beta (sum = new r.r).
-// sc: [bb | rr | alpha | beta], nrhs doubles each.
-__global__ void k_cg_scalars(const double* __restrict__ part, int nblk, int nrhs, int which, double* __restrict__ sc,
-                             int* __restrict__ breakdown) {
+// sc: [bb | rr | alpha | beta], nrhs doubles each.  A column that has met the
+// tolerance (rr <= tol2 bb) is frozen: alpha = beta = 0, so X and R stay as
+// they are, and its p.Ap (rounding noise by then, of either sign) is not
+// taken as a sign that the operator is indefinite.
+__global__ void k_cg_scalars(const double* __restrict__ part, int nblk, int nrhs, int which, double tol2,
+                             double* __restrict__ sc, int* __restrict__ breakdown) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nrhs) return;
   double s = 0.0;
@@ -84,14 +88,16 @@ __global__ void k_cg_scalars(const double* __restrict__ part, int nblk, int nrhs
     bb[c] = s;
     rr[c] = s;
   } else if (which == 1) {
-    if (rr[c] > 0.0 && s > 0.0) {
+    if (rr[c] <= tol2 * bb[c]) {
+      al[c] = 0.0;  // met the tolerance (or a zero residual): frozen
+    } else if (s > 0.0) {
       al[c] = rr[c] / s;
     } else {
       al[c] = 0.0;
-      if (rr[c] > 0.0) *breakdown = 1;  // p.Ap <= 0: the operator is not positive definite
+      *breakdown = 1;  // p.Ap <= 0 on an unconverged column: the operator is not positive definite
     }
   } else {
-    be[c] = rr[c] > 0.0 ? s / rr[c] : 0.0;
+    be[c] = (rr[c] > 0.0 && al[c] != 0.0) ? s / rr[c] : 0.0;
     rr[c] = s;
   }
 }
@@ -146,6 +152,7 @@ struct CgState {
   double *part, *sc;
   int* breakdown;
   unsigned nblk;
+  double tol2;  // a column is done when r.r <= tol2 b.b
 };
 
 // one CG iteration, stream-ordered (no host synchronisation)
@@ -153,9 +160,9 @@ hm_status cg_iteration(const CgState& c, cudaStream_t s) {
   const dim3 grid(c.nblk, c.nrhs);
   HM_TRY(hm_hmatvec(c.h, 0, c.nrhs, c.P, c.n, c.AP, c.n, 0, s));
   k_cg_dot<<<grid, kCgThreads, 0, s>>>(c.P, c.AP, c.n, c.part);
-  k_cg_scalars<<<(c.nrhs + 127) / 128, 128, 0, s>>>(c.part, c.nblk, c.nrhs, 1, c.sc, c.breakdown);
+  k_cg_scalars<<<(c.nrhs + 127) / 128, 128, 0, s>>>(c.part, c.nblk, c.nrhs, 1, c.tol2, c.sc, c.breakdown);
   k_cg_update<<<grid, kCgThreads, 0, s>>>(c.X, c.ldx, c.R, c.P, c.AP, c.n, c.nrhs, c.sc, c.part);
-  k_cg_scalars<<<(c.nrhs + 127) / 128, 128, 0, s>>>(c.part, c.nblk, c.nrhs, 2, c.sc, c.breakdown);
+  k_cg_scalars<<<(c.nrhs + 127) / 128, 128, 0, s>>>(c.part, c.nblk, c.nrhs, 2, c.tol2, c.sc, c.breakdown);
   k_cg_dir<<<grid, kCgThreads, 0, s>>>(c.R, c.P, c.n, c.nrhs, c.sc);
   HM_LAUNCH_CHECK();
   return HM_OK;
@@ -189,10 +196,10 @@ extern "C" hm_status hm_cg_solve(hm_hmatrix h, int nrhs, const float* B, int ldb
   HM_TRY(sc.alloc_async((size_t)4 * nrhs, s));
   HM_TRY(flag.alloc_async(1, s));
   HM_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
-  CgState c{h, n, nrhs, ldx, X, R.p, P.p, AP.p, part.p, sc.p, flag.p, nblk};
+  CgState c{h, n, nrhs, ldx, X, R.p, P.p, AP.p, part.p, sc.p, flag.p, nblk, tol * tol};
   const dim3 grid(nblk, nrhs);
   k_cg_init<<<grid, kCgThreads, 0, s>>>(B, ldb, X, ldx, R.p, P.p, n, part.p);
-  k_cg_scalars<<<(nrhs + 127) / 128, 128, 0, s>>>(part.p, nblk, nrhs, 0, sc.p, flag.p);
+  k_cg_scalars<<<(nrhs + 127) / 128, 128, 0, s>>>(part.p, nblk, nrhs, 0, c.tol2, sc.p, flag.p);
   HM_LAUNCH_CHECK();
 
   std::vector<double> hsc(2 * (size_t)nrhs);  // bb | rr

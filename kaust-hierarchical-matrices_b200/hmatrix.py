@@ -62,6 +62,8 @@ class Stats(ctypes.Structure):
         ("num_unconverged", ctypes.c_longlong),
         ("mixed_bytes", ctypes.c_longlong),
         ("build_seconds", ctypes.c_double),
+        ("num_split", ctypes.c_longlong),
+        ("device_bytes", ctypes.c_longlong),
     ]
 
 
@@ -94,6 +96,9 @@ def lib():
         if hasattr(L, "hm_hmatrix_build"):
             L.hm_build_opts_default.argtypes = [I, ctypes.POINTER(BuildOpts)]
             L.hm_hmatrix_build.argtypes = [P, P, P, ctypes.POINTER(BuildOpts), P, ctypes.POINTER(P)]
+            L.hm_hmatrix_build_rows.argtypes = [P, P, P, ctypes.POINTER(BuildOpts), I, I, P, ctypes.POINTER(P)]
+            L.hm_hmatvec_f64.argtypes = [P, I, I, P, I, P, I, I, P]
+            L.hm_kdtree_build_div.argtypes = [P, I, I, I, I, P, ctypes.POINTER(P)]
             L.hm_hmatrix_stats_get.argtypes = [P, ctypes.POINTER(Stats)]
             L.hm_hmatvec.argtypes = [P, I, I, P, I, P, I, I, P]
             L.hm_hmatrix_free.argtypes = [P]
@@ -298,6 +303,25 @@ class HMatrix:
                                 _stream(stream)))
         return Yc.t()
 
+    def matvec_f64(self, X, Y=None, trans=0, original_order=False, stream=None):
+        """hm_hmatvec_f64: the reference's FP64 vectors, X a float64 CUDA
+        tensor (n, nrhs) with X.T contiguous; narrowed and widened on the
+        device."""
+        import torch
+
+        n = self.n
+        if X.dim() == 1:
+            X = X[:, None]
+        if X.dim() != 2 or X.shape[0] != n or X.dtype != torch.float64 or X.device.type != "cuda":
+            raise ValueError("X must be a float64 CUDA tensor of shape (%d, nrhs)" % n)
+        nrhs = X.shape[1]
+        Xc = X.t().contiguous()
+        Yc = torch.empty((nrhs, n), dtype=torch.float64, device=X.device) if Y is None else Y.t()
+        assert Yc.is_contiguous() and Yc.shape == (nrhs, n)
+        _check(lib().hm_hmatvec_f64(self.h, trans, nrhs, _ptr(Xc), n, _ptr(Yc), n, 1 if original_order else 0,
+                                    _stream(stream)))
+        return Yc.t()
+
     def blocks(self):
         """Host copy of the block list: (lowrank rows [r0, m, c0, n, k, level],
         dense rows [r0, m, c0, n, transposed]), both orientations."""
@@ -439,7 +463,9 @@ def default_opts(d):
 
 def build_hmatrix(tree, structure, points=None, kernel=K_EXP, ell=None, nugget=0.0, tol=1e-5, max_rank=64,
                   leaf_max_rank=0, sample_block=16, precision=PREC_FP32, derivative=0, seed=0, stream=None,
-                  diag_from_coords=-1):
+                  diag_from_coords=-1, leaves=None):
+    """hm_hmatrix_build; with leaves=(leaf_begin, leaf_end), the block-row
+    shard of those leaves' rows (hm_hmatrix_build_rows)."""
     o = default_opts(tree.d)
     o.kernel = kernel
     if ell is not None:
@@ -454,8 +480,12 @@ def build_hmatrix(tree, structure, points=None, kernel=K_EXP, ell=None, nugget=0
     o.seed = seed
     o.diag_from_coords = diag_from_coords
     h = ctypes.c_void_p()
-    _check(lib().hm_hmatrix_build(tree.h, structure.h, _ptr(points) if points is not None else None,
-                                  ctypes.byref(o), _stream(stream), ctypes.byref(h)))
+    pp = _ptr(points) if points is not None else None
+    if leaves is None:
+        _check(lib().hm_hmatrix_build(tree.h, structure.h, pp, ctypes.byref(o), _stream(stream), ctypes.byref(h)))
+    else:
+        _check(lib().hm_hmatrix_build_rows(tree.h, structure.h, pp, ctypes.byref(o), int(leaves[0]),
+                                           int(leaves[1]), _stream(stream), ctypes.byref(h)))
     return HMatrix(h, tree, structure)
 
 

@@ -58,7 +58,9 @@ def test_oracle_library_loads():
 
 
 def test_refcompat_header_compiles(tmp_path):
-    """The reference-name binding (include/hm_refcompat.h) is valid C++ over the C ABI."""
+    """The reference-name binding (include/hm_refcompat.h) is valid C++ over the
+    C ABI, and the reference's main call sequence (tests/refcompat_main.cpp,
+    run on a GPU by test_refcompat_gpu.py) compiles against it."""
     import subprocess
 
     src = tmp_path / "use.cpp"
@@ -68,6 +70,29 @@ def test_refcompat_header_compiles(tmp_path):
     r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(src)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc,
+                        os.path.join(ROOT, "tests", "refcompat_main.cpp")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_division_methods_validate_without_gpu():
+    """hm_kdtree_build_div: an unknown DIVISION_METHOD is HM_ERR_INVALID and
+    POWER_OF_TWO_ON_LEFT on a non-power-of-two n is HM_ERR_UNSUPPORTED, both
+    before any CUDA call."""
+    path = os.path.join(PKG, "libhmb200.so")
+    if not os.path.exists(path):
+        pytest.skip("libhmb200.so not built")
+    lib = ctypes.CDLL(path)
+    lib.hm_last_error.restype = ctypes.c_char_p
+    P, I = ctypes.c_void_p, ctypes.c_int
+    lib.hm_kdtree_build_div.argtypes = [P, I, I, I, I, P, ctypes.POINTER(P)]
+    out = ctypes.c_void_p()
+    assert lib.hm_kdtree_build_div(ctypes.c_void_p(8), 100, 2, 4, 7, None, ctypes.byref(out)) == 1
+    assert b"division" in lib.hm_last_error()
+    assert lib.hm_kdtree_build_div(ctypes.c_void_p(8), 100, 2, 4, 0, None, ctypes.byref(out)) == 4
+    assert b"power-of-two" in lib.hm_last_error()
+    assert out.value is None
 
 
 def test_header_is_plain_c(tmp_path):

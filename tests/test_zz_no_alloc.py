@@ -30,11 +30,26 @@ def hm():
     return hmatrix
 
 
-def _build(hm, n, d, b, tol):
-    pts = hm.generate_dataset(n, d, seed=2024)
+def _build(hm, n, d, b, tol, precision=0, seed=2024):
+    pts = hm.generate_dataset(n, d, seed=seed)
     tree = hm.construct_kdtree(pts, n, d, b)
     st = hm.construct_hmatrix_structure(tree, hm.BOX_CENTER, 1.0)
-    return hm.build_hmatrix(tree, st, pts, kernel=hm.K_MATERN32, ell=0.2, nugget=1e-3, tol=tol, max_rank=64)
+    return hm.build_hmatrix(tree, st, pts, kernel=hm.K_MATERN32, ell=0.2, nugget=1e-3, tol=tol, max_rank=64,
+                            precision=precision)
+
+
+def _compare(hm, H, X, nrhs):
+    """noalloc against hm_hmatvec on the same matrix and X; relative error."""
+    import torch
+
+    L = hm.lib()
+    n = H.n
+    Yref = torch.empty((nrhs, n), device="cuda", dtype=torch.float32)
+    hm._check(L.hm_hmatvec(H.h, 0, nrhs, hm._ptr(X), n, hm._ptr(Yref), n, 0, None))
+    Y = torch.full((nrhs, n), float("nan"), device="cuda", dtype=torch.float32)
+    hm._check(L.hm_hmatvec_noalloc(H.h, nrhs, hm._ptr(X), n, hm._ptr(Y), n, None))
+    torch.cuda.synchronize()
+    return (torch.linalg.norm(Y - Yref) / torch.linalg.norm(Yref)).item()
 
 
 def test_noalloc_matches_hmatvec_twice(hm):
@@ -71,3 +86,34 @@ def test_noalloc_refuses_matrices_beyond_its_scratch(hm):
     assert st == 4  # HM_ERR_UNSUPPORTED
     msg = L.hm_last_error().decode()
     assert "static scratch holds" in msg and "16 MiB" in msg
+
+
+def test_noalloc_mixed_form_after_another_layout(hm):
+    """The mixed form's 16-column passes out of the static array.  A larger
+    matrix with another layout runs first, so its projections, partials and X
+    fragments are what the smaller matrix's calls find in the array: every word
+    they read must be written by their own pass."""
+    import torch
+
+    big = _build(hm, 16384, 3, 64, 1e-4, precision=hm.PREC_MIXED, seed=77)
+    small = _build(hm, 4096, 3, 32, 1e-4, precision=hm.PREC_MIXED)
+    Xb = torch.randn((20, big.n), device="cuda", dtype=torch.float32)
+    assert _compare(hm, big, Xb, 20) < 1e-6
+    Xs = torch.randn((16, small.n), device="cuda", dtype=torch.float32)
+    for nrhs in (16, 16, 3):
+        assert _compare(hm, small, Xs, nrhs) < 1e-6
+
+
+def test_noalloc_refuses_a_mixed_matrix_beyond_its_scratch(hm):
+    """The mixed form needs 16 floats per point for its X fragments, so 2^18
+    points are beyond the 16 MiB array whatever the ranks."""
+    import torch
+
+    n = 1 << 18
+    H = _build(hm, n, 3, 64, 1e-4, precision=hm.PREC_MIXED)
+    L = hm.lib()
+    X = torch.randn((16, n), device="cuda", dtype=torch.float32)
+    Y = torch.empty_like(X)
+    assert L.hm_hmatvec_noalloc(H.h, 16, hm._ptr(X), n, hm._ptr(Y), n, None) == 4
+    msg = L.hm_last_error().decode()
+    assert "mixed form" in msg and "16 per point" in msg and "16 MiB" in msg
