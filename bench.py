@@ -466,8 +466,8 @@ def run_ours(args):
     clocks = ClockSampler(os.path.join(out_dir(), "bench_clocks_%d.csv" % rank))
     res = {}
     for f in forms:
-        # the product runs in passes of 64 right-hand sides (mixed form) or 16 (FP32)
-        width = 64 if f == "mixed" else 16
+        # the product runs in passes of 128 right-hand sides (mixed form) or 16 (FP32)
+        width = 128 if f == "mixed" else 16
         nr = min(width, nrhs)
         panels = (nrhs + width - 1) // width
         ms = timed(step_of(Hs[f]), clocks if f == head else None)
@@ -684,7 +684,7 @@ def run_batch(args):
             _, t = ev_time(lambda: B.build(kernel=kid, ell=w["ell"], nugget=w["nugget"], tol=w["tol"],
                                            max_rank=w["max_rank"], precision=prec, seed=7, stream=s))
             build_s[f] = front_s + t
-            tune[f] = hm.autotune(B.hmatrix(), min(nrhs, 64 if f == "mixed" else 16), cache, stream=s)
+            tune[f] = hm.autotune(B.hmatrix(), min(nrhs, 128 if f == "mixed" else 16), cache, stream=s)
             Bs[f] = B
         head = forms[0]
         N = Bs[head].n
@@ -712,7 +712,7 @@ def run_batch(args):
                 clocks.__exit__()
             ms = ranks.max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
             H = B.hmatrix()
-            width = 64 if f == "mixed" else 16  # right-hand sides per pass of the product
+            width = 128 if f == "mixed" else 16  # right-hand sides per pass of the product
             nr = min(width, nrhs)
             kt = kernel_times(hm, lib, H, X, Y, N, nr, s)
             bp, be = ctypes.c_longlong(), ctypes.c_longlong()

@@ -62,8 +62,9 @@ typedef enum {
 } hm_kernel;
 
 typedef enum {
-  HM_PREC_FP32 = 0,        /* FP32 factors, FP32 arithmetic */
-  HM_PREC_MIXED = 1        /* BF16 factors with a BF16 low part where the tolerance needs it */
+  HM_PREC_FP32 = 0,        /* FP32 factors, FP32 arithmetic (TF32 hi + lo tensor-core products) */
+  HM_PREC_MIXED = 1        /* BF16 factors with a BF16 low part where the tolerance needs it; the FP32
+                              factors are released once the BF16 panels are built */
 } hm_precision;
 
 typedef struct hm_kdtree_s* hm_kdtree;
@@ -226,6 +227,12 @@ typedef struct {
                                 compressed as their four child blocks instead (recursively; at the
                                 leaf level such a block is stored dense) */
   long long device_bytes;    /* device memory the matrix holds now (factors, panels, plans, workspaces) */
+  double phase_seconds[8];   /* wall time of the build's phases (device work charged to the phase that
+                                launched it): [0] set-up of problem lists, batches and workspaces,
+                                [1] sketches Y = A Omega, [2] orthogonalisation and stopping tests,
+                                [3] projections B = A^T Q, [4] truncation (Gram, Jacobi) and factor
+                                packing, [5] diagonal leaf blocks, [6] block lists and factor panels,
+                                [7] the product's plan */
 } hm_hmatrix_stats;
 
 HM_API hm_status hm_hmatrix_stats_get(hm_hmatrix h, hm_hmatrix_stats* st);
@@ -262,17 +269,21 @@ HM_API hm_status hm_hmatvec_f64(hm_hmatrix h, int trans, int nrhs, const double*
  * (4 Mi floats) in the library's device image, held by every GPU that loads
  * the library until the process exits.  It runs passes of 16 right-hand
  * sides, and a pass must fit in the array:
- *   FP32 form:  16 floats per factor column (sum of ranks over both
- *               orientations, padded to 8 per block), plus the chunk partials
- *               of blocks with more than 1024 rows of V;
  *   mixed form: 16 floats per point (X split into BF16 hi + lo fragments,
  *               rows padded to 32 per leaf), plus 128 floats per
  *               (row chunk, 8-column tile) of panels projected in several
  *               row chunks, plus the projections (64 words per 8 factor
- *               columns, 128 for columns with a low part).
- * The 16 floats per point put the mixed form's limit near 2^18 points
- * whatever the ranks.  A matrix beyond the array is rejected with
- * HM_ERR_UNSUPPORTED and a message naming its need.
+ *               columns, 128 for columns with a low part);
+ *   FP32 form on panels (its default product): 32 floats per point (X as
+ *               TF32 hi + lo fragments), the chunk partials as above, plus
+ *               16 floats per factor column (the projections);
+ *   FP32 form with the per-block kernels (schedule "fp32 p1_rows=..."):
+ *               16 floats per factor column (sum of ranks over both
+ *               orientations, padded to 8 per block), plus the chunk partials
+ *               of blocks with more than p1_rows rows of V.
+ * The floats per point put the limit near 2^18 points (mixed) or 2^17 (FP32
+ * on panels) whatever the ranks.  A matrix beyond the array is rejected
+ * with HM_ERR_UNSUPPORTED and a message naming its need.
  *
  * The first call on a device resolves the array's device address on that
  * device (cudaGetSymbolAddress), so make that first call before any stream
@@ -311,8 +322,8 @@ HM_API hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, int 
 HM_API hm_status hm_cg_solve(hm_hmatrix h, int nrhs, const float* B, int ldb, float* X, int ldx, double tol,
                              int max_iter, int check_every, void* stream, int* iterations, double* rel_residual);
 
-/* hm_hmatvec for one pass (nrhs <= 16; <= 64 for the mixed form, whose
- * passes multiply up to four parts of 16 right-hand sides per factor read), X and Y
+/* hm_hmatvec for one pass (nrhs <= 16; <= 128 for the mixed form, whose
+ * passes multiply up to eight parts of 16 right-hand sides per factor read), X and Y
  * in tree order, with CUDA events recorded on `stream`
  * around its two kernels; synchronises and returns each kernel's device time
  * and algorithmic bytes (stored factors and dense blocks read once, X read,
@@ -369,9 +380,11 @@ HM_API hm_status hm_hmatrix_load(hm_kdtree t, hm_structure s, const char* path, 
 
 /* Schedule autotuner (no counterpart in the reference).  Times the product's
  * schedule candidates on this matrix (nrhs columns, at most one pass of the
- * product: 16, or 64 for the mixed form) and keeps the fastest: for the FP32
- * form the rows of V per phase-1 item, for the mixed form the phase-1 unit
- * shape.  With cache_path set, the choice is appended
+ * product: 128 for the mixed form, 16 for the FP32 form) and keeps the
+ * fastest: for the mixed form the phase-1 unit shape and kernel, for the
+ * FP32 form its two products -- FP32 tiles on the factor panels with a
+ * phase-1 unit shape, or the per-block kernels with the rows of V per
+ * phase-1 item.  With cache_path set, the choice is appended
  * to that text file under a key of the GPU and the matrix's shape, and a
  * later call whose key is in the file applies the cached choice without
  * timing (*from_cache = 1).  choice receives a description (may be NULL).
@@ -381,7 +394,9 @@ HM_API hm_status hm_autotune(hm_hmatrix h, int nrhs, const char* cache_path, voi
                              char* choice, int choice_len);
 
 /* Applies a schedule given as hm_autotune describes it, e.g.
- * "mixed chunk_tiles=64 group_tiles=8 p1_ring=1" or "fp32 p1_rows=256". */
+ * "mixed chunk_tiles=64 group_tiles=8 p1_ring=1", "fp32 chunk_tiles=32
+ * group_tiles=4" (FP32 panels) or "fp32 p1_rows=256" (FP32 per-block
+ * kernels; they read the FP32 factors, which FP32 matrices keep). */
 HM_API hm_status hm_schedule_set(hm_hmatrix h, const char* choice, void* stream);
 
 /* --- Batches of independent clouds ------------------------------------------

@@ -1,9 +1,10 @@
 // hm_autotune.cu -- schedule autotuner for the H-matvec, with a file cache.
 //
 // The product's schedule has a few free parameters that change its speed but
-// not what it computes (up to the order of FP32 sums): for the FP32 form the
-// rows of V per phase-1 item, for the mixed form the phase-1 unit shape (row
-// tiles x column tiles).  hm_autotune times every candidate on the matrix at
+// not what it computes (up to the order of FP32 sums): for the mixed form the
+// phase-1 unit shape (row tiles x column tiles) and the phase-1 kernel; for the
+// FP32 form the kernels themselves -- panels with a phase-1 unit shape, or
+// the per-block kernels with the rows of V per phase-1 item.  hm_autotune times every candidate on the matrix at
 // hand with CUDA events, keeps the fastest, and appends it to a cache file
 // under a key made of the GPU and the matrix's shape; a later call with the
 // same key (the same workload on the same GPU) applies the cached choice
@@ -24,23 +25,31 @@ int pass_width(hm_hmatrix h);
 
 namespace {
 
+// mixed: (chunk tiles, group tiles, ring phase 1); FP32 panels: (chunk tiles,
+// group tiles >= 1, 0); FP32 per-block kernels: (p1 rows, 0, 0)
 struct Choice {
-  int a = 0, b = 0, c = 0;  // FP32: (p1 rows, 0, 0); mixed: (chunk tiles, group tiles, ring phase 1)
+  int a = 0, b = 0, c = 0;
 };
+
+bool is_mixed(hm_hmatrix h) { return h->opts.precision == HM_PREC_MIXED; }
 
 std::string describe(hm_hmatrix h, const Choice& c) {
   char buf[96];
-  if (h->mx.enabled)
+  if (is_mixed(h))
     std::snprintf(buf, sizeof buf, "mixed chunk_tiles=%d group_tiles=%d p1_ring=%d", c.a, c.b, c.c);
+  else if (c.b > 0)
+    std::snprintf(buf, sizeof buf, "fp32 chunk_tiles=%d group_tiles=%d", c.a, c.b);
   else
     std::snprintf(buf, sizeof buf, "fp32 p1_rows=%d", c.a);
   return buf;
 }
 
 hm_status apply(hm_hmatrix h, const Choice& c, cudaStream_t s) {
-  if (h->mx.enabled) {
+  if (is_mixed(h) || c.b > 0) {
+    h->mx.enabled = true;
     HM_TRY(mixed_schedule(h, c.a, c.b, c.c, s));
   } else {
+    h->mx.enabled = false;  // the FP32 per-block kernels
     h->plan.p1_rows = c.a;
   }
   return matvec_plan_build(h, 16, s);
@@ -55,7 +64,7 @@ std::string shape_key(hm_hmatrix h, int nrhs) {
   std::string name = pr.name;
   for (char& ch : name)
     if (ch == ' ' || ch == '\t') ch = '_';
-  k << name << "/sm" << pr.multiProcessorCount << "/" << (h->mx.enabled ? "mixed" : "fp32") << "/n" << h->n
+  k << name << "/sm" << pr.multiProcessorCount << "/" << (is_mixed(h) ? "mixed" : "fp32") << "/n" << h->n
     << "/d" << h->d << "/depth" << h->depth << "/lr" << h->stats.num_lowrank << "/ranks" << h->stats.rank_sum
     << "/dense" << h->stats.num_dense << "/nrhs" << nrhs;
   return k.str();
@@ -85,19 +94,21 @@ extern "C" hm_status hm_autotune(hm_hmatrix h, int nrhs, const char* cache_path,
   using namespace hm;
   if (!h) return fail(HM_ERR_INVALID, "hm_autotune: null matrix");
   if (nrhs < 1 || nrhs > pass_width(h))
-    return fail(HM_ERR_INVALID, "hm_autotune: need 1 <= nrhs <= one pass of the product (16, or 64 for the mixed form)");
+    return fail(HM_ERR_INVALID, "hm_autotune: need 1 <= nrhs <= one pass of the product (16, or 128 for the mixed form)");
   cudaStream_t s = as_stream(stream);
   const std::string key = shape_key(h, nrhs);
   Choice best;
   bool cached = cache_path && lookup(cache_path, key, &best);
   if (!cached) {
     std::vector<Choice> cand;
-    if (h->mx.enabled) {
+    if (is_mixed(h)) {
       for (int ring : {1, 0})
         for (int ch : {16, 32, 64, 128})
           for (int g : {4, 8}) cand.push_back(Choice{ch, g, ring});
     } else {
-      for (int r : {128, 256, 512, 1024}) cand.push_back(Choice{r, 0, 0});
+      for (int ch : {16, 32, 64, 128})
+        for (int g : {2, 4}) cand.push_back(Choice{ch, g, 0});
+      for (int r : {256, 1024}) cand.push_back(Choice{r, 0, 0});
     }
     DevBuf<float> X, Y;
     HM_TRY(X.alloc((size_t)h->n * nrhs));
@@ -150,10 +161,14 @@ extern "C" hm_status hm_schedule_set(hm_hmatrix h, const char* choice, void* str
   using namespace hm;
   if (!h || !choice) return fail(HM_ERR_INVALID, "hm_schedule_set: null argument");
   Choice c;
-  if (h->mx.enabled) {
+  if (is_mixed(h)) {
     if (std::sscanf(choice, "mixed chunk_tiles=%d group_tiles=%d p1_ring=%d", &c.a, &c.b, &c.c) != 3)
       return fail(HM_ERR_INVALID, std::string("hm_schedule_set: not a mixed-form schedule: ") + choice);
+  } else if (std::sscanf(choice, "fp32 chunk_tiles=%d group_tiles=%d", &c.a, &c.b) == 2) {
+    if (c.b < 1 || c.b > 8)
+      return fail(HM_ERR_INVALID, std::string("hm_schedule_set: group_tiles must be 1..8: ") + choice);
   } else {
+    c = Choice{};
     if (std::sscanf(choice, "fp32 p1_rows=%d", &c.a) != 1 || c.a < 16)
       return fail(HM_ERR_INVALID, std::string("hm_schedule_set: not an FP32-form schedule: ") + choice);
   }

@@ -1210,7 +1210,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   }
   const long long nprob0 = (long long)probs.size();
 
-  tr.mark("problems", stream);
+  tr.mark("problems", stream, -1, 0);
   // ---- batches bounded by the workspace budget -----------------------------
   size_t freeb = 0, totb = 0;
   HM_CUDA(cudaMemGetInfo(&freeb, &totb));
@@ -1294,7 +1294,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
         if (st0) return st0;
       }
       const int nb = (int)(pend - pstart);
-      tr.mark("batch begin", stream, nb);
+      tr.mark("batch begin", stream, nb, 0);
       std::vector<Prob> bp(probs.begin() + pstart, probs.begin() + pend);
       size_t off = 0;
       std::vector<int2> items_rows, items_cols;
@@ -1383,7 +1383,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
         kf.om_nt = bs8 / 8;
         kf.ws = reinterpret_cast<float*>(ws.p);
       }
-      tr.mark("batch setup", stream, nb);
+      tr.mark("batch setup", stream, nb, 0);
       const int max_rounds = kMaxCols / bs + 2;
       for (int round = 0; round < max_rounds; ++round) {
         if (fast) {
@@ -1404,18 +1404,18 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
           k_kmm<W><<<(unsigned)items_rows.size(), kKmmThreads, kmm_smem<W>(), stream>>>(ka);
         }
         HM_LAUNCH_CHECK();
-        tr.mark("  round sketch", stream, round);
+        tr.mark("  round sketch", stream, round, 1);
         oa.round = round;
         k_orth<W><<<nb, kOrthThreads, orth_smem<W>(), stream>>>(oa);
         HM_LAUNCH_CHECK();
-        tr.mark("  round orth", stream, round);
+        tr.mark("  round orth", stream, round, 2);
         HM_CUDA(cudaMemcpyAsync(hst.data(), dst.p, sizeof(ProbState) * nb, cudaMemcpyDeviceToHost, stream));
         HM_CUDA(cudaStreamSynchronize(stream));
         bool any = false;
         for (auto& x : hst) any |= x.active != 0;
         if (!any) break;
       }
-      tr.mark("sample rounds", stream, nb);
+      tr.mark("sample rounds", stream, nb, 2);
       // B = A^T Q
       DevBuf<uint4> qt;
       DevBuf<long long> dqpoff;
@@ -1430,11 +1430,11 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
         }
         if ((st = qt.alloc_async(std::max<size_t>(qw, 1), stream)) || (st = dqpoff.alloc_async(nb, stream)))
           return st;
-        tr.mark("  q table alloc (MB)", stream, (long long)(qw * 16 >> 20));
+        tr.mark("  q table alloc (MB)", stream, (long long)(qw * 16 >> 20), 3);
         HM_CUDA(cudaMemcpyAsync(dqpoff.p, qpoff.data(), sizeof(long long) * nb, cudaMemcpyHostToDevice, stream));
         k_pack_q<<<nb, 256, 0, stream>>>(dprobs.p, dst.p, reinterpret_cast<const float*>(ws.p), dqpoff.p, qt.p);
         HM_LAUNCH_CHECK();
-        tr.mark("  q pack", stream, nb);
+        tr.mark("  q pack", stream, nb, 3);
         kf.qt = qt.p;
         kf.qpoff = dqpoff.p;
         // one launch per basis-width class, so the narrow (most) blocks run
@@ -1479,7 +1479,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       }
       HM_LAUNCH_CHECK();
 
-      tr.mark("projection", stream, nb);
+      tr.mark("projection", stream, nb, 3);
       // ---- truncation: Gram of B, Jacobi eigen, truncated rank -------------
       HM_CUDA(cudaMemcpyAsync(hst.data(), dst.p, sizeof(ProbState) * nb, cudaMemcpyDeviceToHost, stream));
       HM_CUDA(cudaStreamSynchronize(stream));
@@ -1513,7 +1513,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       HM_CUDA(cudaMemcpyAsync(hst.data(), dst.p, sizeof(ProbState) * nb, cudaMemcpyDeviceToHost, stream));
       HM_CUDA(cudaStreamSynchronize(stream));
 
-      tr.mark("truncation", stream, nb);
+      tr.mark("truncation", stream, nb, 4);
       // ---- results: low rank where converged; otherwise the four child
       // blocks (above the leaf level) or dense (leaf blocks) -----------------
       std::vector<long long> du(nb, -1), dv(nb, -1);
@@ -1618,13 +1618,13 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
           dense_bytes += 8ll * bp[i].m * bp[i].n;
         }
       }
-      tr.mark("factors", stream, nb);
+      tr.mark("factors", stream, nb, 4);
       h->storage.push_back(std::move(chunk));
       pstart = pend;
       if (!children.empty()) {
         probs.insert(probs.end(), children.begin(), children.end());
         grow(probs.size());
-        tr.mark("split into children", stream, (long long)children.size());
+        tr.mark("split into children", stream, (long long)children.size(), 0);
       }
     }
     return HM_OK;
@@ -1672,7 +1672,7 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
     h->storage.push_back(std::move(chunk));
   }
 
-  tr.mark("diagonal leaves", stream);
+  tr.mark("diagonal leaves", stream, -1, 5);
   // ---- block lists (both orientations) --------------------------------------
   const long long nprob = (long long)probs.size();
   for (long long i = 0; i < nprob; ++i) {
@@ -1705,9 +1705,10 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       h->h_dense.push_back(dt);
     }
   }
-  tr.mark("block lists", stream);
-  // ---- mixed precision form -------------------------------------------------
-  if (opt.precision == HM_PREC_MIXED) {
+  tr.mark("block lists", stream, -1, 6);
+  // ---- factor panels: the mixed form's BF16 hi + lo tiles, or the FP32
+  // form's FP32 tiles (both forms multiply on panels) ---------------------------
+  {
     std::vector<MxPair> mp;
     for (long long i = 0; i < nprob; ++i) {
       if (rank[i] <= 0) continue;
@@ -1716,9 +1717,13 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
     }
     std::vector<MxDenseIn> md;
     for (const DenseBlock& db : h->h_dense) md.push_back(MxDenseIn{db.r0, db.m, db.c0, db.n, db.D});
+    h->mx.fmt = opt.precision == HM_PREC_MIXED ? 0 : 1;
     hm_status mst = mixed_build(h, mp, md, stream);
     if (mst) return cleanup(mst);
-    h->stats.mixed_bytes = h->mx.store_tiles * 512;
+    if (opt.precision == HM_PREC_MIXED) {
+      h->stats.mixed_bytes = h->mx.store_tiles * 512;
+      release_fp32(h);
+    }
   }
   h->stats.num_lowrank = lr_count;
   h->stats.num_dense = dense_count;
@@ -1728,10 +1733,11 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   h->stats.dense_bytes = dense_bytes;
   h->stats.num_unconverged = unconverged;
   h->stats.num_split = split_count;
-  tr.mark("mixed panels", stream);
+  tr.mark("mixed panels", stream, -1, 6);
   hm_status st = matvec_plan_build(h, 16, stream);
   if (st) return cleanup(st);
-  tr.mark("matvec plan", stream);
+  tr.mark("matvec plan", stream, -1, 7);
+  for (int i = 0; i < PhaseTrace::kSlots; ++i) h->stats.phase_seconds[i] = tr.sec[i];
   HM_CUDA(cudaEventRecord(ev1, stream));
   HM_CUDA(cudaEventSynchronize(ev1));
   float ms = 0;
@@ -1741,6 +1747,13 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   cudaEventDestroy(ev1);
   *out = h;
   return HM_OK;
+}
+
+void release_fp32(hm_hmatrix_s* h) {
+  h->chunk_meta.clear();
+  for (const auto& c : h->storage) h->chunk_meta.push_back({c.p, c.n});
+  h->storage.clear();
+  h->fp32_released = true;
 }
 
 // Device memory held by the matrix: factor and dense storage, the mixed
@@ -1827,12 +1840,29 @@ hm_status hm_hmatrix_blocks(hm_hmatrix h, long long* num_lowrank, long long* num
   return HM_OK;
 }
 
+// Host copy of an FP32 array of the matrix (a factor or a dense block, count
+// floats): from its storage, or rebuilt from the panels once released.
+static hm_status fetch_fp32(hm_hmatrix h, const float* src, size_t count, float* dst) {
+  if (!count) return HM_OK;
+  if (!h->fp32_released) {
+    HM_CUDA(cudaMemcpy(dst, src, sizeof(float) * count, cudaMemcpyDeviceToHost));
+    return HM_OK;
+  }
+  const int loc = hm::mixed_find_loc(h, src);
+  if (loc < 0) return hm::fail(HM_ERR_INVALID, "no panel holds this block");
+  hm::DevBuf<float> tmp;
+  HM_TRY(tmp.alloc(count));
+  HM_TRY(hm::mixed_unpack(h, {{loc, tmp.p}}, nullptr));
+  HM_CUDA(cudaMemcpy(dst, tmp.p, sizeof(float) * count, cudaMemcpyDeviceToHost));
+  return HM_OK;
+}
+
 hm_status hm_hmatrix_block_factors(hm_hmatrix h, int i, float* U, float* V) {
   if (!h) return hm::fail(HM_ERR_INVALID, "hm_hmatrix_block_factors: null matrix");
   if (i < 0 || (size_t)i >= h->h_lr.size()) return hm::fail(HM_ERR_INVALID, "hm_hmatrix_block_factors: bad index");
   const hm::LRBlock& b = h->h_lr[i];
-  if (U && b.k) HM_CUDA(cudaMemcpy(U, b.U, sizeof(float) * (size_t)b.m * b.k, cudaMemcpyDeviceToHost));
-  if (V && b.k) HM_CUDA(cudaMemcpy(V, b.V, sizeof(float) * (size_t)b.n * b.k, cudaMemcpyDeviceToHost));
+  if (U && b.k) HM_TRY(fetch_fp32(h, b.U, (size_t)b.m * b.k, U));
+  if (V && b.k) HM_TRY(fetch_fp32(h, b.V, (size_t)b.n * b.k, V));
   return HM_OK;
 }
 
@@ -1840,7 +1870,7 @@ hm_status hm_hmatrix_dense_block(hm_hmatrix h, int i, float* D) {
   if (!h) return hm::fail(HM_ERR_INVALID, "hm_hmatrix_dense_block: null matrix");
   if (i < 0 || (size_t)i >= h->h_dense.size()) return hm::fail(HM_ERR_INVALID, "hm_hmatrix_dense_block: bad index");
   const hm::DenseBlock& b = h->h_dense[i];
-  if (D && b.m && b.n) HM_CUDA(cudaMemcpy(D, b.D, sizeof(float) * (size_t)b.m * b.n, cudaMemcpyDeviceToHost));
+  if (D && b.m && b.n) HM_TRY(fetch_fp32(h, b.D, (size_t)b.m * b.n, D));
   return HM_OK;
 }
 

@@ -90,6 +90,9 @@ struct MatvecPlan {
 struct hm_hmatrix_s;
 namespace hm {
 long long device_bytes(const hm_hmatrix_s* h);
+// Frees the FP32 factor and dense storage of a mixed-form matrix whose panels
+// are built (their address ranges stay in chunk_meta).
+void release_fp32(hm_hmatrix_s* h);
 }  // namespace hm
 
 struct hm_hmatrix_s {
@@ -99,6 +102,12 @@ struct hm_hmatrix_s {
   hm_build_opts opts{};
   hm::KernelParams kp{};
   std::vector<hm::DevBuf<float>> storage;  // factor / dense chunks
+  // The mixed form releases its FP32 chunks once its BF16 panels are built
+  // (the product reads the panels only); what the chunks held is then rebuilt
+  // from the panels when asked for (export, files).  chunk_meta keeps each
+  // released chunk's address range, the identity of the arrays in it.
+  bool fp32_released = false;
+  std::vector<std::pair<const float*, size_t>> chunk_meta;
   hm_hmatrix_stats stats{};
   hm::MatvecPlan plan;
   hm::MxPlan mx;                     // mixed precision form (panels of BF16 hi + lo tiles)

@@ -36,28 +36,34 @@ hm_status cuda_fail(cudaError_t e, const char* what, const char* file, int line)
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // ---- phase trace --------------------------------------------------------------
-// With HM_TRACE=1 in the environment, a build prints the wall-clock time of
-// each phase to stderr (the stream is synchronised at every mark, so device
-// work is charged to the phase that launched it).  Off, a mark costs nothing.
+// A build marks the end of each phase: the stream is synchronised at the
+// mark, so device work is charged to the phase that launched it, and the
+// wall-clock time since the previous mark is added to the phase's slot (the
+// marks sit where the build waits for the device anyway, so this costs a few
+// milliseconds per build).  With HM_TRACE=1 in the environment every mark is
+// also printed to stderr.
 struct PhaseTrace {
+  static constexpr int kSlots = 8;
   bool on = false;
   const char* what = "";
+  double sec[kSlots] = {};
   std::chrono::steady_clock::time_point last;
   explicit PhaseTrace(const char* w) : what(w) {
     const char* e = std::getenv("HM_TRACE");
     on = e != nullptr && e[0] != '\0' && e[0] != '0';
     last = std::chrono::steady_clock::now();
   }
-  void mark(const char* phase, cudaStream_t s, long long arg = -1) {
-    if (!on) return;
+  void mark(const char* phase, cudaStream_t s, long long arg = -1, int slot = 0) {
     cudaStreamSynchronize(s);
     const auto now = std::chrono::steady_clock::now();
     const double ms = std::chrono::duration<double, std::milli>(now - last).count();
+    if (slot >= 0 && slot < kSlots) sec[slot] += ms * 1e-3;
+    last = now;
+    if (!on) return;
     if (arg >= 0)
       std::fprintf(stderr, "[hm trace] %s %-24s %5lld %10.3f ms\n", what, phase, arg, ms);
     else
       std::fprintf(stderr, "[hm trace] %s %-24s       %10.3f ms\n", what, phase, ms);
-    last = now;
   }
 };
 

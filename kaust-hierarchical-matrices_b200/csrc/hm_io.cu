@@ -21,6 +21,7 @@
 //   the chunks' floats, in order
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <new>
 #include <vector>
@@ -98,12 +99,18 @@ extern "C" hm_status hm_hmatrix_save(hm_hmatrix h, const char* path) {
                                     "the whole matrix");
   // every stored pair sits in h_lr as (block, mirror) at 2i, 2i + 1
   if (h->h_lr.size() % 2) return fail(HM_ERR_UNSUPPORTED, "hm_hmatrix_save: unpaired block list");
+  // the storage chunks, or, once the mixed form released them, their ranges
+  std::vector<std::pair<const float*, size_t>> chunks = h->chunk_meta;
+  if (!h->fp32_released) {
+    chunks.clear();
+    for (const DevBuf<float>& b : h->storage) chunks.push_back({b.p, b.n});
+  }
   auto locate = [&](const float* p, int32_t* c, int64_t* o) {
-    for (size_t i = 0; i < h->storage.size(); ++i) {
-      const DevBuf<float>& b = h->storage[i];
-      if (p >= b.p && p < b.p + b.n) {
+    for (size_t i = 0; i < chunks.size(); ++i) {
+      const float* base = chunks[i].first;
+      if (std::less_equal<const float*>()(base, p) && std::less<const float*>()(p, base + chunks[i].second)) {
         *c = (int32_t)i;
-        *o = (int64_t)(p - b.p);
+        *o = (int64_t)(p - base);
         return true;
       }
     }
@@ -145,10 +152,10 @@ extern "C" hm_status hm_hmatrix_save(hm_hmatrix h, const char* path) {
   put(&h->opts, sizeof h->opts);
   put(&h->stats, sizeof h->stats);
   put(&fp, sizeof fp);
-  const int64_t nch = (int64_t)h->storage.size();
+  const int64_t nch = (int64_t)chunks.size();
   put(&nch, sizeof nch);
-  for (const DevBuf<float>& b : h->storage) {
-    const uint64_t nf = b.n;
+  for (const auto& c : chunks) {
+    const uint64_t nf = c.second;
     put(&nf, sizeof nf);
   }
   const int64_t np = (int64_t)pairs.size(), nd = (int64_t)dense.size();
@@ -157,12 +164,35 @@ extern "C" hm_status hm_hmatrix_save(hm_hmatrix h, const char* path) {
   put(&nd, sizeof nd);
   put(dense.data(), sizeof(DenseRec) * dense.size());
   std::vector<float> stage((size_t)1 << 24);  // 64 MiB at a time
-  for (const DevBuf<float>& b : h->storage)
-    for (size_t o = 0; ok && o < b.n; o += stage.size()) {
-      const size_t c = std::min(stage.size(), b.n - o);
-      HM_CUDA(cudaMemcpy(stage.data(), b.p + o, sizeof(float) * c, cudaMemcpyDeviceToHost));
+  // released chunks: every factor and dense block of a chunk rebuilt from the
+  // panels into a device copy of the chunk (values that convert back to the
+  // same tiles), then written like a stored chunk
+  std::vector<std::vector<std::pair<int, int64_t>>> per_chunk(chunks.size());  // (h_locs index, offset)
+  if (h->fp32_released)
+    for (size_t i = 0; i < h->mx.h_locs.size(); ++i) {
+      int32_t c = 0;
+      int64_t o = 0;
+      if (!locate(h->mx.h_locs[i].key, &c, &o))
+        return fail(HM_ERR_UNSUPPORTED, "hm_hmatrix_save: a panel block outside the matrix's storage");
+      per_chunk[c].push_back({(int)i, o});
+    }
+  for (size_t ci = 0; ci < chunks.size() && ok; ++ci) {
+    const float* src = chunks[ci].first;
+    DevBuf<float> rebuilt;
+    if (h->fp32_released) {
+      HM_TRY(rebuilt.alloc(std::max<size_t>(chunks[ci].second, 1)));
+      HM_CUDA(cudaMemset(rebuilt.p, 0, sizeof(float) * chunks[ci].second));
+      std::vector<std::pair<int, float*>> jobs;
+      for (const auto& lo : per_chunk[ci]) jobs.push_back({lo.first, rebuilt.p + lo.second});
+      HM_TRY(mixed_unpack(h, jobs, nullptr));
+      src = rebuilt.p;
+    }
+    for (size_t o = 0; ok && o < chunks[ci].second; o += stage.size()) {
+      const size_t c = std::min(stage.size(), chunks[ci].second - o);
+      HM_CUDA(cudaMemcpy(stage.data(), src + o, sizeof(float) * c, cudaMemcpyDeviceToHost));
       put(stage.data(), sizeof(float) * c);
     }
+  }
   if (!ok) return fail(HM_ERR_INVALID, std::string("hm_hmatrix_save: write to ") + path + " failed");
   if (std::fclose(out.f) != 0) {
     out.f = nullptr;
@@ -301,10 +331,12 @@ hm_status load_impl(hm_kdtree t, hm_structure s, const char* path, void* stream,
     mp.push_back(MxPair{r.level, r.r0, r.m, r.c0, r.n, r.k, r.khi, b.U, b.V});
   }
   for (const DenseRec& r : dense) h->h_dense.push_back(DenseBlock{r.r0, r.m, r.c0, r.n, 0, at(r.c, r.o)});
-  if (h->opts.precision == HM_PREC_MIXED) {
+  {
     std::vector<MxDenseIn> md;
     for (const DenseBlock& db : h->h_dense) md.push_back(MxDenseIn{db.r0, db.m, db.c0, db.n, db.D});
+    h->mx.fmt = h->opts.precision == HM_PREC_MIXED ? 0 : 1;
     HM_TRY(mixed_build(h.get(), mp, md, st));
+    if (h->opts.precision == HM_PREC_MIXED) release_fp32(h.get());  // as the build does
   }
   HM_TRY(matvec_plan_build(h.get(), 16, st));
   HM_CUDA(cudaStreamSynchronize(st));

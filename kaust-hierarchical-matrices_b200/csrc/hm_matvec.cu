@@ -36,8 +36,8 @@ static __device__ __align__(256) float hm_noalloc_scratch[size_t(4) << 20];
 namespace hm {
 
 // Right-hand sides per pass of the product: the mixed form reads every factor
-// tile once for up to four parts of 16, the FP32 form runs 16 at a time.
-int pass_width(hm_hmatrix h) { return h->mx.enabled ? 64 : 16; }
+// tile once for up to eight parts of 16, the FP32 form runs 16 at a time.
+int pass_width(hm_hmatrix h) { return h->mx.enabled && h->mx.fmt == 0 ? 128 : 16; }
 
 namespace {
 
@@ -491,9 +491,11 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream) {
   HM_TRY(P.dense.alloc(std::max<size_t>(h->h_dense.size(), 1)));
   HM_TRY(P.leaf_dptr.alloc(nleaf + 1));
   HM_TRY(P.leaf_dblk.alloc(dblk.size()));
-  // projection scratch of one pass, for whichever form runs (the mixed form
-  // runs passes of up to 64 right-hand sides, the FP32 form 16)
-  const long long scratch = h->mx.enabled ? h->mx.scratch_floats(4) : tk + part;
+  // projection scratch of one pass, for whichever product runs (the mixed
+  // form's panels: passes of up to 128 right-hand sides; the FP32 form's
+  // panels or per-block kernels: 16)
+  const long long scratch =
+      h->mx.enabled ? h->mx.scratch_floats(h->mx.fmt == 0 ? 8 : 1) : tk + part;
   HM_TRY(P.T.alloc(std::max<long long>(scratch, 1)));
   HM_TRY(P.Xp.alloc((size_t)h->n * pass_width(h)));
   HM_TRY(P.Yp.alloc((size_t)h->n * pass_width(h)));
@@ -661,10 +663,12 @@ extern "C" hm_status hm_hmatvec_noalloc(hm_hmatrix h, int nrhs, const float* X, 
   const size_t need = h->mx.enabled ? (size_t)h->mx.scratch_floats() : (size_t)P.t_floats + (size_t)P.part_floats;
   if (need > hm::kNoallocScratchFloats) {
     const std::string what =
-        h->mx.enabled ? " floats of scratch for a 16-column pass of the mixed form (16 per point for the X "
-                        "fragments, plus chunk partials and projections)"
-                      : " floats of projection scratch for a 16-column pass of the FP32 form (16 per factor "
-                        "column, plus chunk partials)";
+        !h->mx.enabled ? " floats of projection scratch for a 16-column pass of the FP32 form's per-block product "
+                         "(16 per factor column, plus chunk partials)"
+        : h->mx.fmt == 0 ? " floats of scratch for a 16-column pass of the mixed form (16 per point for the X "
+                           "fragments, plus chunk partials and projections)"
+                         : " floats of scratch for a 16-column pass of the FP32 form (32 per point for the X "
+                           "fragments, plus chunk partials and projections)";
     return hm::fail(HM_ERR_UNSUPPORTED, "hm_hmatvec_noalloc: this matrix needs " + std::to_string(need) + what +
                                             "; the static scratch holds " +
                                             std::to_string(hm::kNoallocScratchFloats) + " (16 MiB)");
@@ -698,7 +702,7 @@ extern "C" hm_status hm_hmatvec_profile(hm_hmatrix h, int nrhs, const float* X, 
                                         long long* bytes_project, long long* bytes_expand) {
   if (!h) return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: null matrix");
   if (nrhs < 1 || nrhs > hm::pass_width(h) || !X || !Y || ldx < h->n || ldy < h->n)
-    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: need 1 <= nrhs <= one pass (16, or 64 for the mixed "
+    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_profile: need 1 <= nrhs <= one pass (16, or 128 for the mixed "
                                     "form) and valid vectors");
   cudaStream_t s = hm::as_stream(stream);
   hm::KernelMarks km;
@@ -724,7 +728,7 @@ extern "C" hm_status hm_hmatvec_kernels(hm_hmatrix h, int nrhs, const float* X, 
                                         int* count) {
   if (!h) return hm::fail(HM_ERR_INVALID, "hm_hmatvec_kernels: null matrix");
   if (nrhs < 1 || nrhs > hm::pass_width(h) || !X || !Y || ldx < h->n || ldy < h->n || cap < 0)
-    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_kernels: need 1 <= nrhs <= one pass (16, or 64 for the mixed "
+    return hm::fail(HM_ERR_INVALID, "hm_hmatvec_kernels: need 1 <= nrhs <= one pass (16, or 128 for the mixed "
                                     "form) and valid vectors");
   hm::KernelMarks km;
   HM_TRY(hm::timed_panel(h, nrhs, X, ldx, Y, ldy, hm::as_stream(stream), &km));

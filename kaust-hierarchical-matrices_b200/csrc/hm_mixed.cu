@@ -56,6 +56,15 @@ __device__ __forceinline__ uint4 ld_keep(const uint4* ptr, uint64_t pol) {
   return v;
 }
 
+// A factor tile: streamed past the caches (evict-first) when one warp reads
+// it; through L1 when the warps of a CTA all read it (each for its own
+// right-hand sides), so that the siblings of the first reader hit in L1.
+template <bool SHARED>
+__device__ __forceinline__ uint4 ld_tile(const uint4* p) {
+  if (SHARED) return __ldg(p);
+  return __ldcs(p);
+}
+
 // T layout, per panel: its nctl tiles with low parts, then the others.
 //   with low parts (128 words): lane (g,t) x {column 2t at right-hand sides g,
 //     g + 8; column 2t + 1 at g, g + 8}, each word bf16x2 {hi, lo}
@@ -151,7 +160,7 @@ __global__ void __launch_bounds__(128) k_mx_split_x(const float* __restrict__ X,
 // per step, NH: halves of 16 right-hand sides (each V tile is loaded once for
 // both); a half's X fragments, S and T sit xh, sh and th elements after the
 // previous half's.
-template <int NCT, int RU, int NH>
+template <int NCT, int RU, int NH, bool SH = false>
 __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, const uint4* __restrict__ store,
                                            const uint4* __restrict__ Xf, const int* __restrict__ tslot,
                                            float4* __restrict__ S, uint32_t* __restrict__ T, long long xh,
@@ -182,8 +191,8 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
       const uint4* lp = store + (P.lo1 + rt * P.nctl + u.ct0) * 32 + lane;
 #pragma unroll
       for (int j = 0; j < NCT; ++j) {
-        vh[q][j] = ok && j < u.nct ? __ldcs(hp + j * 32) : z;
-        vl[q][j] = ok && j < u.nct && u.ct0 + j < P.nctl ? __ldcs(lp + j * 32) : z;
+        vh[q][j] = ok && j < u.nct ? ld_tile<SH>(hp + j * 32) : z;
+        vl[q][j] = ok && j < u.nct && u.ct0 + j < P.nctl ? ld_tile<SH>(lp + j * 32) : z;
       }
     }
 #pragma unroll
@@ -231,19 +240,29 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
   }
 }
 
-// One warp per CTA, 16 per SM (measured): a warp runs one unit and retires at
-// once, instead of holding its CTA's slot until three sibling warps with
-// other units finish; 16 warps keep enough loads in flight at 128 registers.
-constexpr int kP1Warps = 1, kP1PerSm = 16;
-template <int NH>
-__global__ void __launch_bounds__(32 * kP1Warps, kP1PerSm / kP1Warps) k_mx_p1(const MxUnit* __restrict__ units, int nunits,
+// One unit per CTA.  WPC = 1: one warp per CTA, 16 per SM (measured): a warp
+// runs one unit and retires at once, instead of holding its CTA's slot until
+// sibling warps with other units finish; 16 warps keep enough loads in flight
+// at 128 registers.  WPC > 1 (passes of more than 64 right-hand sides): the
+// CTA's warps take the same unit, warp w parts w NH .. w NH + NH - 1, and
+// share its factor tiles through L1.
+constexpr int kP1PerSm = 16;
+template <int NH, int WPC>
+__global__ void __launch_bounds__(32 * WPC, kP1PerSm / WPC) k_mx_p1(const MxUnit* __restrict__ units, int nunits,
                                                const MxPanel* __restrict__ panels, const uint4* __restrict__ store,
                                                const uint4* __restrict__ Xf, const int* __restrict__ tslot,
                                                float4* __restrict__ S, uint32_t* __restrict__ T, long long xh,
                                                long long sh, long long th) {
-  const int w = blockIdx.x * kP1Warps + (threadIdx.x >> 5);
+  const int w = blockIdx.x;
   if (w >= nunits) return;
   const int lane = threadIdx.x & 31;
+  constexpr bool SH = WPC > 1;
+  if (SH) {  // this warp's parts
+    const int h0 = (threadIdx.x >> 5) * NH;
+    Xf += h0 * xh;
+    S += h0 * sh;
+    T += h0 * th;
+  }
   const MxUnit u = units[w];
   const MxPanel P = panels[u.panel];
   if (NH == 1) {
@@ -258,7 +277,7 @@ __global__ void __launch_bounds__(32 * kP1Warps, kP1PerSm / kP1Warps) k_mx_p1(co
       MxUnit a = u;
       a.ct0 = u.ct0 + c;
       a.nct = min(2, u.nct - c);
-      mx_p1_unit<2, 1, NH>(a, P, store, Xf, tslot, S, T, xh, sh, th, lane);
+      mx_p1_unit<2, 1, NH, SH>(a, P, store, Xf, tslot, S, T, xh, sh, th, lane);
     }
   } else if (u.nct > 2) {  // two halves: at most four column tiles at a time
     MxUnit a = u;
@@ -478,9 +497,11 @@ __device__ __forceinline__ void mx_p2_step_hi(float (&acc)[2][2][4], const uint4
 // flight, and a warp that finishes its row tile frees its slot at once)
 // With two halves of 16 right-hand sides every U tile is loaded once for both,
 // and the warp holds twice the accumulators (16 warps per SM, 128 registers).
-constexpr int kP2Warps = 1, kP2PerSm = 28, kP2PerSm2 = 16;
-template <int NH>
-__global__ void __launch_bounds__(32 * kP2Warps, (NH == 1 ? kP2PerSm : kP2PerSm2) / kP2Warps)
+// WPC > 1 (passes of more than 32 right-hand sides): the CTA's warps take the
+// same row tile, warp w parts w NH .., and share its factor tiles through L1.
+constexpr int kP2PerSm = 28, kP2PerSm2 = 16;
+template <int NH, int WPC>
+__global__ void __launch_bounds__(32 * WPC, (NH == 1 ? kP2PerSm : kP2PerSm2) / WPC)
     k_mx_p2(int tile0, int tile_end, int depth, const int* __restrict__ tile_leaf,
                                                const int* __restrict__ leaf_tile0, const int* __restrict__ leaf_off,
                                                const int* __restrict__ pan_of, const MxPanel* __restrict__ panels,
@@ -489,9 +510,17 @@ __global__ void __launch_bounds__(32 * kP2Warps, (NH == 1 ? kP2PerSm : kP2PerSm2
                                                const MxDense* __restrict__ dense, const uint4* __restrict__ Xf,
                                                float* __restrict__ Y, int ldy, int nr, long long xh_, long long th) {
   // global row tiles [tile0, tile_end): every tile, or a block-row shard's
-  const int G = tile0 + blockIdx.x * kP2Warps + (threadIdx.x >> 5);
+  const int G = tile0 + blockIdx.x;
   if (G >= tile_end) return;
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  constexpr bool SH = WPC > 1;
+  if (SH) {  // this warp's parts
+    const int h0 = (threadIdx.x >> 5) * NH;
+    T += h0 * th;
+    Xf += h0 * xh_;
+    Y += (size_t)16 * h0 * ldy;
+    nr -= 16 * h0;
+  }
   const int x = tile_leaf[G];
   float acc[NH][2][2][4];
 #pragma unroll
@@ -535,10 +564,10 @@ __global__ void __launch_bounds__(32 * kP2Warps, (NH == 1 ? kP2PerSm : kP2PerSm2
 #pragma unroll 2
     for (int ct = 0; ct < nctl; ct += 2) {
       const bool two = ct + 1 < nctl;
-      const uint4 h0 = __ldcs(uh + ct * 32);
-      const uint4 h1 = two ? __ldcs(uh + (ct + 1) * 32) : z;
-      const uint4 l0 = __ldcs(ul + ct * 32);
-      const uint4 l1 = two ? __ldcs(ul + (ct + 1) * 32) : z;
+      const uint4 h0 = ld_tile<SH>(uh + ct * 32);
+      const uint4 h1 = two ? ld_tile<SH>(uh + (ct + 1) * 32) : z;
+      const uint4 l0 = ld_tile<SH>(ul + ct * 32);
+      const uint4 l1 = two ? ld_tile<SH>(ul + (ct + 1) * 32) : z;
 #pragma unroll
       for (int h = 0; h < NH; ++h) {
         const uint4 t0 = __ldg(tl + h * (th >> 2) + ct * 32);
@@ -556,8 +585,8 @@ __global__ void __launch_bounds__(32 * kP2Warps, (NH == 1 ? kP2PerSm : kP2PerSm2
 #pragma unroll 2
     for (int ct = nctl; ct < nct; ct += 2) {
       const bool two = ct + 1 < nct;
-      const uint4 h0 = __ldcs(uh + ct * 32);
-      const uint4 h1 = two ? __ldcs(uh + (ct + 1) * 32) : z;
+      const uint4 h0 = ld_tile<SH>(uh + ct * 32);
+      const uint4 h1 = two ? ld_tile<SH>(uh + (ct + 1) * 32) : z;
 #pragma unroll
       for (int h = 0; h < NH; ++h) {
         const uint2 w0 = __ldg(tw + h * (th >> 1) + (ct - nctl) * 32);
@@ -574,8 +603,8 @@ __global__ void __launch_bounds__(32 * kP2Warps, (NH == 1 ? kP2PerSm : kP2PerSm2
     const uint4* dh = store + (D.hi + rt * D.nct) * 32 + lane;
     const uint4* dl = store + (D.lo + rt * D.nct) * 32 + lane;
     for (int ct = 0; ct < D.nct; ct += 2) {
-      const uint4 h0 = __ldcs(dh + ct * 32), h1 = __ldcs(dh + (ct + 1) * 32);
-      const uint4 l0 = __ldcs(dl + ct * 32), l1 = __ldcs(dl + (ct + 1) * 32);
+      const uint4 h0 = ld_tile<SH>(dh + ct * 32), h1 = ld_tile<SH>(dh + (ct + 1) * 32);
+      const uint4 l0 = ld_tile<SH>(dl + ct * 32), l1 = ld_tile<SH>(dl + (ct + 1) * 32);
       const size_t xt = (size_t)(D.col_tile0 + (ct >> 2)) * 128 + (size_t)((ct >> 1) & 1) * 32 + lane;
 #pragma unroll
       for (int h = 0; h < NH; ++h) {
@@ -708,6 +737,10 @@ hm_status upload(DevBuf<T>& b, const std::vector<T>& v, cudaStream_t s) {
 hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const std::vector<MxDenseIn>& dense_in,
                       cudaStream_t s) {
   MxPlan& M = h->mx;
+  // FP32 format: no low parts, 1 KB tiles (two 512-byte units), T indexed by
+  // global column (128 words per 8-column tile)
+  const bool f32 = M.fmt == 1;
+  const int tu = f32 ? 2 : 1;  // 512-byte units per tile
   const int depth = h->depth;
   const std::vector<int>& lo = h->tree->h_offsets;
   const int nleaf = 1 << depth;
@@ -776,17 +809,19 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   for (int p = 0; p < np; ++p) {
     long long sl = 0, sh_ = 0;
     for (const Side& m : members[p]) {
-      sl += pairs[m.pair].khi;
-      sh_ += pairs[m.pair].k - pairs[m.pair].khi;
+      const int kl = f32 ? 0 : pairs[m.pair].khi;
+      sl += kl;
+      sh_ += pairs[m.pair].k - kl;
     }
     const int KL = (int)((sl + 7) / 8 * 8), KH = (int)((sh_ + 7) / 8 * 8);
     long long al = 0, ah = KL;
     for (const Side& m : members[p]) {
       const MxPair& q = pairs[m.pair];
+      const int kl = f32 ? 0 : q.khi;
       (m.side ? colL_v : colL_u)[m.pair] = (int)al;
       (m.side ? colH_v : colH_u)[m.pair] = (int)ah;
-      al += q.khi;
-      ah += q.k - q.khi;
+      al += kl;
+      ah += q.k - kl;
     }
     MxPanel& P = panels[p];
     const int sh = depth - plevel[p];
@@ -797,22 +832,22 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
     P.nrt = leaf_tile0[x1] - P.tile0;
     P.r0 = lo[x0];
     P.hi1 = tiles;
-    tiles += (long long)P.nrt * P.nct;
+    tiles += (long long)P.nrt * P.nct * tu;
     P.lo1 = tiles;
     tiles += (long long)P.nrt * P.nctl;
     P.hi2 = tiles;
-    tiles += (long long)P.nrt * P.nct;
+    tiles += (long long)P.nrt * P.nct * tu;
     P.lo2 = tiles;
     tiles += (long long)P.nrt * P.nctl;
     P.t0 = t_tiles;
     t_tiles += P.nct;
     P.tw0 = t_words;
-    t_words += (long long)P.nctl * 128 + (long long)(P.nct - P.nctl) * 64;
+    t_words += f32 ? (long long)P.nct * 128 : (long long)P.nctl * 128 + (long long)(P.nct - P.nctl) * 64;
   }
 
   // column sources and the projection's column map
-  if ((long long)t_tiles * 8 > 0x7fffffffll || t_words >= (1ll << 30))
-    return fail(HM_ERR_UNSUPPORTED, "mixed form: too many factor columns");
+  if ((long long)t_tiles * 8 > 0x7fffffffll || (!f32 && t_words >= (1ll << 30)))
+    return fail(HM_ERR_UNSUPPORTED, "panel form: too many factor columns");
   std::vector<const float*> colsrc((size_t)t_tiles * 8, nullptr);
   std::vector<int> mirror((size_t)t_tiles * 8, -1);  // partner column (an involution)
   long long bytes_lr = 0;
@@ -821,15 +856,25 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
     if (q.k <= 0) continue;
     const int pu = panel_u[i], pv = panel_v[i];
     const long long bu = panels[pu].t0 * 8, bv = panels[pv].t0 * 8;
+    const int kl = f32 ? 0 : q.khi;
     for (int c = 0; c < q.k; ++c) {
-      const int cu = c < q.khi ? colL_u[i] + c : colH_u[i] + c - q.khi;
-      const int cv = c < q.khi ? colL_v[i] + c : colH_v[i] + c - q.khi;
+      const int cu = c < kl ? colL_u[i] + c : colH_u[i] + c - kl;
+      const int cv = c < kl ? colL_v[i] + c : colH_v[i] + c - kl;
       colsrc[bu + cu] = q.fu + (size_t)c * q.m;
       colsrc[bv + cv] = q.fv + (size_t)c * q.n;
       mirror[bv + cv] = (int)(bu + cu);  // Y_u += fu (fv^T X_v)
       mirror[bu + cu] = (int)(bv + cv);  // Y_v += fv (fu^T X_u)
     }
-    bytes_lr += 2ll * (q.m + q.n) * (q.k + q.khi);
+    bytes_lr += f32 ? 4ll * (q.m + q.n) * q.k : 2ll * (q.m + q.n) * (q.k + q.khi);
+  }
+  std::vector<MxLoc> locs;
+  locs.reserve(2 * pairs.size() + dense_in.size());
+  for (size_t i = 0; i < pairs.size(); ++i) {
+    const MxPair& q = pairs[i];
+    if (q.k <= 0) continue;
+    const int kl = f32 ? 0 : q.khi;
+    locs.push_back(MxLoc{q.fu, 0, panel_u[i], q.m, q.k, kl, colL_u[i], colH_u[i]});
+    locs.push_back(MxLoc{q.fv, 0, panel_v[i], q.n, q.k, kl, colL_v[i], colH_v[i]});
   }
 
 
@@ -853,10 +898,11 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
     D.n = di.n;
     D.src = di.D;
     D.hi = tiles;
-    tiles += (long long)D.nrt * D.nct;
+    tiles += (long long)D.nrt * D.nct * tu;
     D.lo = tiles;
-    tiles += (long long)D.nrt * D.nct;
+    if (!f32) tiles += (long long)D.nrt * D.nct;
     for (int x = xs; x < xe; ++x) leaf_d[x].push_back((int)dense.size());
+    locs.push_back(MxLoc{di.D, 1, (int)dense.size(), di.m, di.n, 0, 0, 0});
     dense.push_back(D);
     bytes_dense += 4ll * di.m * di.n;
   }
@@ -875,10 +921,13 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   HM_TRY(upload(M.pan_of, pan_of, s));
   HM_TRY(upload(M.tile_leaf, tile_leaf, s));
   HM_TRY(upload(M.leaf_tile0, leaf_tile0, s));
-  std::vector<int> own(mirror.size()), tslot(mirror.size());  // (word << 1) | no-low-part
+  // BF16 format: (word << 1) | no-low-part of the destination; FP32 format:
+  // the destination's global column (its T words follow from it)
+  std::vector<int> own(mirror.size()), tslot(mirror.size());
   for (const MxPanel& P : panels)
     for (int c = 0; c < P.nct * 8; ++c)
-      own[P.t0 * 8 + c] = (int)(t_word(P.tw0, P.nctl, c) << 1) | ((c >> 3) >= P.nctl ? 1 : 0);
+      own[P.t0 * 8 + c] = f32 ? (int)(P.t0 * 8 + c)
+                              : (int)(t_word(P.tw0, P.nctl, c) << 1) | ((c >> 3) >= P.nctl ? 1 : 0);
   for (size_t c = 0; c < mirror.size(); ++c) tslot[c] = mirror[c] >= 0 ? own[mirror[c]] : -1 - own[c];
   HM_TRY(upload(M.tslot, tslot, s));
   HM_TRY(upload(M.dense, dense, s));
@@ -886,6 +935,9 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   HM_TRY(upload(M.leaf_dblk, dblk, s));
   M.num_panels = np;
   M.num_dense = (int)dense.size();
+  M.h_dense = dense;
+  M.h_locs = std::move(locs);
+  M.loc_index.clear();
   M.t_tiles = t_tiles;
   M.t_words = t_words;
   // each factor is read once per phase (as V of one orientation in phase 1,
@@ -893,6 +945,12 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   M.bytes_p1 = bytes_lr;
   M.bytes_p2 = bytes_lr + bytes_dense;
 
+  if (f32) {
+    HM_TRY(fp32_convert(h, colsrc, dense, s));
+    HM_CUDA(cudaStreamSynchronize(s));
+    M.enabled = true;
+    return HM_OK;
+  }
   DevBuf<const float*> dcol;
   DevBuf<long long> dstart;
   if (np > 0) {
@@ -932,8 +990,128 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   return HM_OK;
 }
 
+namespace {
+
+struct UnpackJob {
+  int kind, idx, rows, cols, khi, colL, colH;
+  float* dst;
+};
+
+// row R (tree order) -> its global 32-row tile and the row within it
+__device__ __forceinline__ void row_tile(const int* __restrict__ leaf_off, const int* __restrict__ leaf_tile0,
+                                         int nleaf, int R, int* G, int* rr) {
+  int lo = 0, hi = nleaf - 1;  // the leaf x with leaf_off[x] <= R < leaf_off[x + 1]
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (leaf_off[mid] <= R)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  *G = leaf_tile0[lo] + (R - leaf_off[lo]) / 32;
+  *rr = (R - leaf_off[lo]) % 32;
+}
+
+// element (rr, cc) of a P2-order BF16 tile at unit `tile`, as a float
+__device__ __forceinline__ float p2_elem(const uint4* __restrict__ store, long long tile, int rr, int cc) {
+  const int lane = 4 * (rr & 7) + (cc >> 1), comp = rr >> 3;
+  const uint32_t w = reinterpret_cast<const uint32_t*>(store + tile * 32 + lane)[comp];
+  return (cc & 1) ? bf16_hi_as_float(w) : bf16_lo_as_float(w);
+}
+
+__global__ void k_mx_unpack(const UnpackJob* __restrict__ jobs, const long long* __restrict__ start, int njobs,
+                            long long total, const MxPanel* __restrict__ panels, const MxDense* __restrict__ dense,
+                            const uint4* __restrict__ store, const int* __restrict__ leaf_off,
+                            const int* __restrict__ leaf_tile0, int nleaf) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= total) return;
+  const int j = find_item(start, njobs, e);
+  const UnpackJob J = jobs[j];
+  const long long local = e - start[j];
+  const int r = (int)(local % J.rows), c = (int)(local / J.rows);
+  int G, rr, ct, cc;
+  long long thi, tlo = -1;
+  if (J.kind == 0) {
+    const MxPanel P = panels[J.idx];
+    row_tile(leaf_off, leaf_tile0, nleaf, P.r0 + r, &G, &rr);
+    const int pc = c < J.khi ? J.colL + c : J.colH + c - J.khi;
+    ct = pc >> 3;
+    cc = pc & 7;
+    thi = P.hi2 + (long long)(G - P.tile0) * P.nct + ct;
+    if (ct < P.nctl) tlo = P.lo2 + (long long)(G - P.tile0) * P.nctl + ct;
+  } else {
+    const MxDense D = dense[J.idx];
+    row_tile(leaf_off, leaf_tile0, nleaf, D.r0 + r, &G, &rr);
+    int GC, cr;
+    row_tile(leaf_off, leaf_tile0, nleaf, D.c0 + c, &GC, &cr);
+    const int pc = (GC - D.col_tile0) * 32 + cr;
+    ct = pc >> 3;
+    cc = pc & 7;
+    thi = D.hi + (long long)(G - D.row_tile0) * D.nct + ct;
+    tlo = D.lo + (long long)(G - D.row_tile0) * D.nct + ct;
+  }
+  const float hi = p2_elem(store, thi, rr, cc);
+  float y = hi;
+  if (tlo >= 0) {
+    const float lo = p2_elem(store, tlo, rr, cc);
+    y = hi + lo;  // exact: hi + lo has at most 24 significant bits
+    // a tie (|lo| half a BF16 ulp of hi) would round to the other neighbour
+    if (bf16_lo_as_float(pack_bf16(y, 0.f)) != hi) y = nextafterf(y, hi);
+  }
+  J.dst[(size_t)c * J.rows + r] = y;
+}
+
+}  // namespace
+
+int mixed_find_loc(hm_hmatrix_s* h, const float* key) {
+  MxPlan& M = h->mx;
+  if (M.loc_index.size() != M.h_locs.size()) {
+    M.loc_index.resize(M.h_locs.size());
+    for (size_t i = 0; i < M.h_locs.size(); ++i) M.loc_index[i] = {M.h_locs[i].key, (int)i};
+    std::sort(M.loc_index.begin(), M.loc_index.end(),
+              [](const std::pair<const float*, int>& a, const std::pair<const float*, int>& b) {
+                return std::less<const float*>()(a.first, b.first);
+              });
+  }
+  auto it = std::lower_bound(M.loc_index.begin(), M.loc_index.end(), std::make_pair(key, -1),
+                             [](const std::pair<const float*, int>& a, const std::pair<const float*, int>& b) {
+                               return std::less<const float*>()(a.first, b.first);
+                             });
+  return (it != M.loc_index.end() && it->first == key) ? it->second : -1;
+}
+
+hm_status mixed_unpack(hm_hmatrix_s* h, const std::vector<std::pair<int, float*>>& jobs, cudaStream_t s) {
+  MxPlan& M = h->mx;
+  if (jobs.empty()) return HM_OK;
+  if (M.fmt != 0) return fail(HM_ERR_UNSUPPORTED, "panel unpack: FP32 panels keep their FP32 factors");
+  std::vector<UnpackJob> uj;
+  std::vector<long long> start;
+  long long tot = 0;
+  for (const auto& jb : jobs) {
+    if (jb.first < 0 || (size_t)jb.first >= M.h_locs.size())
+      return fail(HM_ERR_INVALID, "panel unpack: unknown factor");
+    const MxLoc& L = M.h_locs[jb.first];
+    if ((long long)L.rows * L.cols == 0) continue;
+    uj.push_back(UnpackJob{L.kind, L.idx, L.rows, L.cols, L.khi, L.colL, L.colH, jb.second});
+    start.push_back(tot);
+    tot += (long long)L.rows * L.cols;
+  }
+  if (tot == 0) return HM_OK;
+  DevBuf<UnpackJob> dj;
+  DevBuf<long long> ds;
+  HM_TRY(upload(dj, uj, s));
+  HM_TRY(upload(ds, start, s));
+  k_mx_unpack<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(dj.p, ds.p, (int)uj.size(), tot, M.panels.p, M.dense.p,
+                                                            M.store.p, h->tree->offsets.p, M.leaf_tile0.p,
+                                                            1 << h->depth);
+  HM_LAUNCH_CHECK();
+  HM_CUDA(cudaStreamSynchronize(s));
+  return HM_OK;
+}
+
 hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, int p1_ring, cudaStream_t s) {
   MxPlan& M = h->mx;
+  if (M.fmt == 1) p1_ring = 0;  // the ring variant exists for the BF16 format only
   if (p1_ring) {
     int dev = 0;
     HM_CUDA(cudaGetDevice(&dev));
@@ -981,11 +1159,11 @@ hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, int 
 hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, float* scratch,
                           cudaStream_t s, KernelMarks* km) {
   MxPlan& M = h->mx;
-  if (nr < 1 || nr > 64) return fail(HM_ERR_INVALID, "mixed product: a pass holds 1 to 64 right-hand sides");
-  // 16-column parts of this pass: 1, 2 or 4 (a pass of 33-48 runs four, the
-  // last one zero)
-  const int nh = nr > 32 ? 4 : (nr > 16 ? 2 : 1);
-  // scratch: the halves' X fragments, then their chunk partials, then their T
+  if (M.fmt == 1) return fp32_run_panel(h, nr, X, ldx, Y, ldy, scratch, s, km);
+  if (nr < 1 || nr > 128) return fail(HM_ERR_INVALID, "mixed product: a pass holds 1 to 128 right-hand sides");
+  // 16-column parts of this pass: 1, 2, 4 or 8 (the parts past nr are zero)
+  const int nh = nr > 64 ? 8 : (nr > 32 ? 4 : (nr > 16 ? 2 : 1));
+  // scratch: the parts' X fragments, then their chunk partials, then their T
   const long long xh = (long long)M.num_tiles * 128, sh = M.s_tiles * 32, th = M.t_words;
   uint4* Xf = reinterpret_cast<uint4*>(scratch);
   float4* S = reinterpret_cast<float4*>(Xf + nh * xh);
@@ -999,6 +1177,7 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
     if (km) km->mark("k_mx_split_x", 4ll * h->n * nr + xbytes, s);
   }
   if (M.num_units > 0) {
+    const unsigned nu = (unsigned)M.num_units;
     if (M.p1_ring && nh == 1 && M.group_tiles <= 4) {
       k_mx_p1r<8, 3, 4><<<M.num_sms, 256, ring_smem<8, 3, 4>(), s>>>(M.units.p, M.num_units, M.panels.p, M.store.p,
                                                                       Xf, M.tslot.p, S, T);
@@ -1006,14 +1185,13 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
       k_mx_p1r<4, 4, 8><<<M.num_sms, 128, ring_smem<4, 4, 8>(), s>>>(M.units.p, M.num_units, M.panels.p, M.store.p,
                                                                       Xf, M.tslot.p, S, T);
     } else if (nh == 1) {
-      k_mx_p1<1><<<(M.num_units + kP1Warps - 1) / kP1Warps, 32 * kP1Warps, 0, s>>>(
-          M.units.p, M.num_units, M.panels.p, M.store.p, Xf, M.tslot.p, S, T, xh, sh, th);
+      k_mx_p1<1, 1><<<nu, 32, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf, M.tslot.p, S, T, xh, sh, th);
     } else if (nh == 2) {
-      k_mx_p1<2><<<(M.num_units + kP1Warps - 1) / kP1Warps, 32 * kP1Warps, 0, s>>>(
-          M.units.p, M.num_units, M.panels.p, M.store.p, Xf, M.tslot.p, S, T, xh, sh, th);
-    } else {
-      k_mx_p1<4><<<(M.num_units + kP1Warps - 1) / kP1Warps, 32 * kP1Warps, 0, s>>>(
-          M.units.p, M.num_units, M.panels.p, M.store.p, Xf, M.tslot.p, S, T, xh, sh, th);
+      k_mx_p1<2, 1><<<nu, 32, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf, M.tslot.p, S, T, xh, sh, th);
+    } else if (nh == 4) {
+      k_mx_p1<4, 1><<<nu, 32, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf, M.tslot.p, S, T, xh, sh, th);
+    } else {  // eight parts: two warps of four parts share each unit's tiles
+      k_mx_p1<4, 2><<<nu, 64, 0, s>>>(M.units.p, M.num_units, M.panels.p, M.store.p, Xf, M.tslot.p, S, T, xh, sh, th);
     }
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_mx_p1", M.bytes_p1 + xbytes, s);
@@ -1025,23 +1203,20 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
     if (km) km->mark("k_mx_reduce", (512ll * M.s_tiles + 512ll * M.nmt) * nh, s);
   }
   if (M.p2_tiles > 0) {
-    const unsigned grid = (unsigned)((M.p2_tiles + kP2Warps - 1) / kP2Warps);
+    const unsigned grid = (unsigned)M.p2_tiles;
     const int te = M.p2_tile0 + M.p2_tiles;
+#define HM_P2_ARGS                                                                                            \
+  M.p2_tile0, te, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off, M.pan_of.p, M.panels.p, M.store.p, T,      \
+      M.leaf_dptr.p, M.leaf_dblk.p, M.dense.p, Xf, Y, ldy, nr, xh, th
     if (nh == 1)
-      k_mx_p2<1><<<grid, 32 * kP2Warps, 0, s>>>(M.p2_tile0, te, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
-                                                M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p, M.leaf_dblk.p,
-                                                M.dense.p, Xf, Y, ldy, nr, xh, th);
+      k_mx_p2<1, 1><<<grid, 32, 0, s>>>(HM_P2_ARGS);
     else if (nh == 2)
-      k_mx_p2<2><<<grid, 32 * kP2Warps, 0, s>>>(M.p2_tile0, te, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
-                                                M.pan_of.p, M.panels.p, M.store.p, T, M.leaf_dptr.p, M.leaf_dblk.p,
-                                                M.dense.p, Xf, Y, ldy, nr, xh, th);
-    else  // four parts: two launches of two parts each (a four-part phase 2 spills
-          // at 128 registers and measured slower than two of these)
-      for (int q = 0; q < 2 && nr > 32 * q; ++q)
-        k_mx_p2<2><<<grid, 32 * kP2Warps, 0, s>>>(M.p2_tile0, te, h->depth, M.tile_leaf.p, M.leaf_tile0.p, leaf_off,
-                                                  M.pan_of.p, M.panels.p, M.store.p, T + 2 * q * th, M.leaf_dptr.p,
-                                                  M.leaf_dblk.p, M.dense.p, Xf + 2 * q * xh, Y + (size_t)32 * q * ldy,
-                                                  ldy, std::min(32, nr - 32 * q), xh, th);
+      k_mx_p2<2, 1><<<grid, 32, 0, s>>>(HM_P2_ARGS);
+    else if (nh == 4)  // two warps of two parts share each row tile's factor tiles
+      k_mx_p2<2, 2><<<grid, 64, 0, s>>>(HM_P2_ARGS);
+    else  // four warps of two parts
+      k_mx_p2<2, 4><<<grid, 128, 0, s>>>(HM_P2_ARGS);
+#undef HM_P2_ARGS
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_mx_p2", M.bytes_p2 + xbytes + 4ll * h->n * nr, s);
   }

@@ -54,8 +54,20 @@ struct MxDense {  // a dense block in P2 order, hi + lo, [row tile][col tile]
   const float* src;          // the FP32 block (m x n, column-major); read only while converting
 };
 
+// Where one FP32 factor (or dense block) of the matrix sits in the panels:
+// the columns of a pair's side in its cluster's panel (the first khi of them
+// in the low-part group at colL, the others at colH), or a dense block.
+struct MxLoc {
+  const float* key;  // the FP32 array it was converted from (its identity, also after that array is freed)
+  int kind;          // 0 factor, 1 dense block
+  int idx;           // panel, or dense block
+  int rows, cols;    // rows x columns, column-major, as the FP32 array was
+  int khi, colL, colH;
+};
+
 struct MxPlan {
-  bool enabled = false;
+  bool enabled = false;  // the product runs on the panels (else the FP32 per-block kernels)
+  int fmt = 0;           // tile format: 0 BF16 hi + lo (mixed form), 1 FP32 in TF32 fragment order (FP32 form)
   DevBuf<uint4> store;  // all BF16 tiles
   long long store_tiles = 0;
   DevBuf<MxPanel> panels;
@@ -82,15 +94,19 @@ struct MxPlan {
   DevBuf<int> leaf_dptr, leaf_dblk;  // dense blocks covering each leaf's rows
   long long bytes_p1 = 0, bytes_p2 = 0;  // BF16 bytes of the factors (unpadded) and dense blocks
   std::vector<MxPanel> h_panels;          // host copy (the schedule rebuilds units and S offsets)
+  std::vector<MxDense> h_dense;           // host copy
+  std::vector<MxLoc> h_locs;              // every factor and dense block converted into the panels
+  std::vector<std::pair<const float*, int>> loc_index;  // h_locs by key, sorted (built on first use)
   int chunk_tiles = 128, group_tiles = 4;  // phase-1 unit shape (schedule parameters)
   bool p1_ring = false;                    // phase 1 by persistent warps with a cp.async ring
   int num_sms = 148;
   // scratch of one 16-column panel of right-hand sides, in floats: X
   // fragments, chunk partials, T (the projections by expanding column: BF16
   // hi + lo for the columns with low parts, hi for the others)
-  // of a pass of `halves` such panels (1, 2 or 4: up to 64 right-hand sides)
+  // of a pass of `halves` such panels (1, 2, 4 or 8: up to 128 right-hand sides)
+  // (FP32 format: X as TF32 hi + lo, 8 words per lane and tile instead of 4)
   long long scratch_floats(int halves = 1) const {
-    return (((long long)num_tiles * 4 + s_tiles) * 128 + t_words) * halves;
+    return (((long long)num_tiles * (fmt ? 8 : 4) + s_tiles) * 128 + t_words) * halves;
   }
 };
 
@@ -118,11 +134,28 @@ struct KernelMarks;
 // matvec plan afterwards (the scratch size changes).
 hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, int p1_ring, cudaStream_t s);
 
-// One pass of nr <= 64 right-hand sides in tree order (two or four parts of 16
+// One pass of nr <= 128 right-hand sides in tree order (two, four or eight parts of 16
 // when nr > 16: every factor tile is read once for all of them); scratch holds
-// scratch_floats(h) floats, h = 1, 2 or 4 parts.  km (optional) receives an event
+// scratch_floats(h) floats, h = 1, 2, 4 or 8 parts.  km (optional) receives an event
 // after each kernel.
 hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, float* scratch,
                           cudaStream_t s, KernelMarks* km);
+
+// The FP32 values of the BF16 panels: for each (h_locs index, device
+// destination), the factor or dense block rebuilt column-major from its hi
+// (+ lo) tiles.  A value is hi + lo (exact in FP32), moved one FP32 ulp toward
+// hi where hi + lo would round to another BF16 hi, so that converting the
+// result again gives the same tiles bit for bit.
+hm_status mixed_unpack(hm_hmatrix_s* h, const std::vector<std::pair<int, float*>>& jobs, cudaStream_t s);
+
+// Index into h_locs of the factor or dense block converted from `key`, or -1.
+int mixed_find_loc(hm_hmatrix_s* h, const float* key);
+
+// The FP32 format (hm_fp32.cu): tile conversion of the panels and dense
+// blocks, and one pass of nr <= 16 right-hand sides.
+hm_status fp32_convert(hm_hmatrix_s* h, const std::vector<const float*>& colsrc, const std::vector<MxDense>& dense,
+                       cudaStream_t s);
+hm_status fp32_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, float* scratch,
+                         cudaStream_t s, KernelMarks* km);
 
 }  // namespace hm

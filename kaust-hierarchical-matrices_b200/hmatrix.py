@@ -64,7 +64,10 @@ class Stats(ctypes.Structure):
         ("build_seconds", ctypes.c_double),
         ("num_split", ctypes.c_longlong),
         ("device_bytes", ctypes.c_longlong),
+        ("phase_seconds", ctypes.c_double * 8),
     ]
+
+    PHASES = ("setup", "sketch", "orth", "projection", "truncation", "diagonal", "panels", "plan")
 
 
 _lib = None
@@ -278,7 +281,9 @@ class HMatrix:
     def stats(self):
         st = Stats()
         _check(lib().hm_hmatrix_stats_get(self.h, ctypes.byref(st)))
-        return {k: getattr(st, k) for k, _ in Stats._fields_}
+        out = {k: getattr(st, k) for k, _ in Stats._fields_ if k != "phase_seconds"}
+        out["phase_seconds"] = dict(zip(Stats.PHASES, list(st.phase_seconds)))
+        return out
 
     def matvec(self, X, Y=None, trans=0, original_order=False, stream=None):
         """Y = H X for a float32 CUDA tensor X of shape (n, nrhs), column-major

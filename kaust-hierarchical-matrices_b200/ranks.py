@@ -75,6 +75,7 @@ def subtree_shards(leaf_offsets, world):
     as contiguous runs, one run per rank, each run ending at the subtree
     boundary nearest to an equal share of the rows.  Returns one tuple
     (leaf_begin, leaf_end, row_begin, row_end) per rank."""
+    leaf_offsets = [int(x) for x in leaf_offsets]
     nleaf = len(leaf_offsets) - 1
     depth = int(round(math.log2(nleaf)))
     if (1 << depth) != nleaf:

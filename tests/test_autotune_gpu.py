@@ -87,3 +87,31 @@ def test_batching_workload_full_size(hm, tmp_path):
         Yref = oracle.dense_rows_matvec(pts.cpu().numpy(), n, 3, perm, oracle.K_EXP, 0.1, 0.0, rows, Xc.T).T
         err = np.linalg.norm(Yb[r0:r1][rows] - Yref) / np.linalg.norm(Yref)
         assert err < 20 * 1e-5, (c, n, err)
+
+
+def test_fp32_panels_match_the_per_block_kernels(hm):
+    """The FP32 form has two products: FP32 tiles on the factor panels (the
+    default) and the per-block kernels; both are 3xTF32, so they agree to FP32
+    rounding, in tree and in original order and over several passes."""
+    import torch
+
+    n = 1 << 16
+    pts = hm.generate_dataset(n, 3, seed=21)
+    tree = hm.construct_kdtree(pts, n, 3, 64)
+    st = hm.construct_hmatrix_structure(tree, hm.BOX_CENTER, 1.0)
+    H = hm.build_hmatrix(tree, st, pts, kernel=hm.K_EXP, ell=0.2, tol=1e-6, max_rank=128)
+    X = torch.randn((n, 37), device="cuda").t().contiguous().t()
+    for order in (False, True):
+        hm.schedule_set(H, "fp32 chunk_tiles=32 group_tiles=4")
+        Yp = H.matvec(X, original_order=order)
+        hm.schedule_set(H, "fp32 p1_rows=512")
+        Yb = H.matvec(X, original_order=order)
+        rel = (torch.linalg.norm(Yp - Yb) / torch.linalg.norm(Yb)).item()
+        assert rel < 1e-6, (order, rel)
+    perm = tree.copy_out()["perm"]
+    rows = np.random.default_rng(3).choice(n, 128, replace=False)
+    hm.schedule_set(H, "fp32 chunk_tiles=128 group_tiles=2")
+    Y = H.matvec(X[:, :5]).cpu().numpy()
+    Yref = oracle.dense_rows_matvec(pts.cpu().numpy(), n, 3, perm, oracle.K_EXP, 0.2, 0.0, rows,
+                                    X[:, :5].t().cpu().numpy().astype(np.float64)).T
+    assert np.linalg.norm(Y[rows] - Yref) / np.linalg.norm(Yref) < 5e-6

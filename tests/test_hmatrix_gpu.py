@@ -214,6 +214,36 @@ def test_mixed_precision_matvec(hm, n, d, b):
     np.testing.assert_array_equal(Hm.matvec(Xd, trans=1).cpu().numpy(), Y)
 
 
+def test_mixed_form_holds_no_fp32_factors(hm):
+    """A mixed-form matrix keeps its BF16 panels only: the FP32 factors and
+    dense blocks it was converted from are released after the build.  Factors
+    and dense blocks exported from it are rebuilt from the panels (the
+    per-block tolerance check above reads them that way), and converting
+    them again gives the same panels (the file round trip is bit-identical,
+    test_io_gpu)."""
+    import torch
+
+    n, d, b = 20000, 3, 64
+    kind, ell, nugget, tol = hm.K_MATERN32, 0.2, 1e-3, 1e-4
+    pts, tree, st, Hm = build(hm, n, d, b, kind, ell, tol, 128, nugget=nugget, seed=11, precision=hm.PREC_MIXED)
+    s = Hm.stats()
+    # beyond the panels only the product's workspaces remain (projection
+    # scratch for 128 right-hand sides, the per-pass X and Y copies): less than
+    # the FP32 factors alone would take
+    assert s["device_bytes"] - s["mixed_bytes"] < s["factor_bytes"], s
+    # a dense block read back is the kernel to BF16 hi + lo accuracy
+    _, dense = Hm.blocks()
+    perm = tree.copy_out()["perm"]
+    import ctypes
+
+    r0, m, c0, nc, _ = (int(x) for x in dense[0])
+    D = np.zeros(m * nc, np.float32)
+    hm._check(hm.lib().hm_hmatrix_dense_block(Hm.h, 0, D.ctypes.data_as(ctypes.c_void_p)))
+    Dref = oracle.dense_block(pts, n, d, perm, kind, ell, nugget, r0, m, c0, nc)
+    err = np.linalg.norm(D.reshape(nc, m).T - Dref) / np.linalg.norm(Dref)
+    assert err < 1e-5, err
+
+
 def _profile_bytes(hm, H, n):
     import ctypes
     import torch
@@ -248,11 +278,13 @@ def test_mixed_moves_fewer_bytes_and_agrees_with_fp32(hm):
 
 @pytest.mark.parametrize("diag_from_coords", [0, 1])
 def test_mixed_two_half_passes_match_single_passes(hm, diag_from_coords):
-    """The mixed form multiplies up to 32 right-hand sides per pass: two halves
-    of 16 share every factor tile read.  A 40-column product (a pass of 32 and
-    one of 8) equals the same columns multiplied 16, 16 and 8 at a time, in
-    tree order and in the points' original order, with the diagonal blocks
-    stored or generated from coordinates."""
+    """The mixed form multiplies up to 128 right-hand sides per pass: parts of
+    16 share every factor tile read (two or four parts per warp; beyond 64
+    right-hand sides, and in phase 2 beyond 32, the warps of a CTA share the
+    tiles).  Products of 40 (four parts) and 100 columns (eight parts) equal
+    the same columns multiplied 16 at a time, in tree order and in the points'
+    original order, with the diagonal blocks stored or generated from
+    coordinates."""
     import torch
 
     n, d, b = 24000, 3, 64
@@ -262,11 +294,12 @@ def test_mixed_two_half_passes_match_single_passes(hm, diag_from_coords):
     st = hm.construct_hmatrix_structure(tree, hm.BOX_CENTER, 1.0)
     H = hm.build_hmatrix(tree, st, pts, kernel=kind, ell=ell, nugget=nugget, tol=tol, max_rank=128,
                          precision=hm.PREC_MIXED, diag_from_coords=diag_from_coords)
-    X = torch.randn((40, n), device="cuda", dtype=torch.float32).t()
-    for orig in (False, True):
-        Y = H.matvec(X, original_order=orig)
-        parts = [H.matvec(X[:, c0:c1].t().contiguous().t(), original_order=orig) for c0, c1 in
-                 ((0, 16), (16, 32), (32, 40))]
-        Ys = torch.cat(parts, dim=1)
-        scale = torch.linalg.norm(Ys).item()
-        assert torch.linalg.norm(Y - Ys).item() <= 1e-6 * scale
+    for ncol in (40, 100):
+        X = torch.randn((ncol, n), device="cuda", dtype=torch.float32).t()
+        for orig in (False, True):
+            Y = H.matvec(X, original_order=orig)
+            parts = [H.matvec(X[:, c0:min(c0 + 16, ncol)].t().contiguous().t(), original_order=orig)
+                     for c0 in range(0, ncol, 16)]
+            Ys = torch.cat(parts, dim=1)
+            scale = torch.linalg.norm(Ys).item()
+            assert torch.linalg.norm(Y - Ys).item() <= 1e-6 * scale, (ncol, orig)
