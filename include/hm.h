@@ -206,7 +206,9 @@ HM_API hm_status hm_hmatrix_build(hm_kdtree t, hm_structure s, const double* d_p
  * Its product (hm_hmatvec, hm_hmatvec_f64) reads all of X and writes only
  * the shard's rows of Y: the other rows are left untouched.  Stacking the
  * shards' rows gives the whole matrix's product.  Same tree, structure and
- * options as hm_hmatrix_build; a shard cannot be saved to a file. */
+ * options as hm_hmatrix_build.  A shard saved to a file (hm_hmatrix_save)
+ * loads back as the same shard: the pieces of an out-of-core product, built
+ * and applied one at a time (hmatrix.PiecewiseHMatrix). */
 HM_API hm_status hm_hmatrix_build_rows(hm_kdtree t, hm_structure s, const double* d_points,
                                        const hm_build_opts* opts, int leaf_begin, int leaf_end, void* stream,
                                        hm_hmatrix* out);

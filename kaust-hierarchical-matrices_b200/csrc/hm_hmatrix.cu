@@ -1039,6 +1039,15 @@ __global__ void k_pack_trunc(const Prob* probs, const ProbState* st, const W* ws
   const int k = st[p].k, r = st[p].r;
   if (dst_u[p] < 0 || r <= 0) return;
   const Prob P = probs[p];
+  if (k > kTruncMax) {  // kept as sampled (W = I): U = Q, V = B, a copy
+    for (int side = 0; side < 2; ++side) {
+      const size_t cnt = (size_t)(side ? P.n : P.m) * r;
+      const W* src = ws + (side ? P.boff : P.qoff);
+      float* out = dst + (side ? dst_v[p] : dst_u[p]);
+      for (size_t e = threadIdx.x; e < cnt; e += blockDim.x) out[e] = (float)src[e];
+    }
+    return;
+  }
   const float* w = Wr + goff[p];
   __shared__ float ws_sh[kMaxCols * 32];
   const int rc = min(r, 32);
@@ -1387,7 +1396,11 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       const int max_rounds = kMaxCols / bs + 2;
       for (int round = 0; round < max_rounds; ++round) {
         if (fast) {
-          const int rbs = (round == 0 ? bs0 : bs) + bst;  // basis + test columns
+          // basis + test columns: double width in the first round and again
+          // from the third on (the blocks still active by then are the
+          // high-rank ones; entry generation, not the sample width, is the
+          // cost of a round, so wider rounds mean fewer of them)
+          const int rbs = (round == 1 ? bs : bs0) + bst;
           k_omega_pack<<<592, 256, 0, stream>>>(om2.p, om_rows2 / 8, rbs, bs8 / 8, ka.seed, round);
           HM_LAUNCH_CHECK();
           kf.round = round;

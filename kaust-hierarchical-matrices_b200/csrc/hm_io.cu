@@ -36,7 +36,7 @@ hm_status matvec_plan_build(hm_hmatrix h, int nrhs_cap, cudaStream_t stream);
 namespace {
 
 constexpr char kMagic[8] = {'H', 'M', 'B', '2', '0', '0', 'H', '1'};
-constexpr uint32_t kVersion = 1;
+constexpr uint32_t kVersion = 2;  // 2: the block-row range (leaves) after the dimensions
 
 uint64_t fnv(uint64_t hsh, const void* p, size_t bytes) {
   const unsigned char* c = static_cast<const unsigned char*>(p);
@@ -94,9 +94,6 @@ struct DenseRec {
 extern "C" hm_status hm_hmatrix_save(hm_hmatrix h, const char* path) {
   using namespace hm;
   if (!h || !path) return fail(HM_ERR_INVALID, "hm_hmatrix_save: null argument");
-  if (h->leaf_lo != 0 || h->leaf_hi != (1 << h->depth))
-    return fail(HM_ERR_UNSUPPORTED, "hm_hmatrix_save: a block-row shard is saved as part of no file format; save "
-                                    "the whole matrix");
   // every stored pair sits in h_lr as (block, mirror) at 2i, 2i + 1
   if (h->h_lr.size() % 2) return fail(HM_ERR_UNSUPPORTED, "hm_hmatrix_save: unpaired block list");
   // the storage chunks, or, once the mixed form released them, their ranges
@@ -146,9 +143,11 @@ extern "C" hm_status hm_hmatrix_save(hm_hmatrix h, const char* path) {
   };
   const uint32_t vers[3] = {kVersion, (uint32_t)sizeof(hm_build_opts), (uint32_t)sizeof(hm_hmatrix_stats)};
   const int32_t dims[4] = {h->n, h->d, h->depth, h->diag_fly ? 1 : 0};
+  const int32_t leaves[2] = {h->leaf_lo, h->leaf_hi};  // the whole matrix, or a block-row shard
   put(kMagic, 8);
   put(vers, sizeof vers);
   put(dims, sizeof dims);
+  put(leaves, sizeof leaves);
   put(&h->opts, sizeof h->opts);
   put(&h->stats, sizeof h->stats);
   put(&fp, sizeof fp);
@@ -234,18 +233,19 @@ hm_status load_impl(hm_kdtree t, hm_structure s, const char* path, void* stream,
   auto bad = [&](const std::string& why) { return fail(HM_ERR_INVALID, "hm_hmatrix_load: " + why + ": " + path); };
   char magic[8];
   uint32_t vers[3];
-  int32_t dims[4];
+  int32_t dims[4], leaves[2];
   if (!get(magic, 8) || std::memcmp(magic, kMagic, 8) != 0) return bad("not an H-matrix file");
   if (!get(vers, sizeof vers) || vers[0] != kVersion || vers[1] != sizeof(hm_build_opts) ||
       vers[2] != sizeof(hm_hmatrix_stats))
     return bad("written by another version of the library");
   std::unique_ptr<hm_hmatrix_s> h(new hm_hmatrix_s());
   uint64_t fp = 0, mine = 0;
-  if (!get(dims, sizeof dims) || !get(&h->opts, sizeof h->opts) || !get(&h->stats, sizeof h->stats) ||
-      !get(&fp, sizeof fp))
+  if (!get(dims, sizeof dims) || !get(leaves, sizeof leaves) || !get(&h->opts, sizeof h->opts) ||
+      !get(&h->stats, sizeof h->stats) || !get(&fp, sizeof fp))
     return bad("truncated header");
   if (dims[0] != t->n || dims[1] != t->d || dims[2] != t->depth)
     return bad("the tree's size or depth differs from the one the matrix was built on");
+  if (leaves[0] < 0 || leaves[0] >= leaves[1] || leaves[1] > (1 << t->depth)) return bad("bad block-row range");
   HM_TRY(fingerprint(t, s, &mine));
   if (mine != fp) return bad("the tree or structure differs from the one the matrix was built on");
   int64_t nch = 0;
@@ -287,8 +287,8 @@ hm_status load_impl(hm_kdtree t, hm_structure s, const char* path, void* stream,
   h->n = t->n;
   h->d = t->d;
   h->depth = t->depth;
-  h->leaf_lo = 0;
-  h->leaf_hi = 1 << t->depth;
+  h->leaf_lo = leaves[0];
+  h->leaf_hi = leaves[1];
   h->diag_fly = dims[3] != 0;
   h->kp.kind = h->opts.kernel;
   h->kp.deriv = h->opts.derivative ? 1 : 0;

@@ -21,8 +21,9 @@
 // BF16 rounding is within the budget) gets T's hi only: one word holds
 // right-hand sides g and g + 8, and phase 2 multiplies U_hi T_hi alone.
 // Each product of a BF16 pair uses three MMAs (hi*lo, lo*hi, hi*hi; lo*lo is
-// below FP32 rounding); the low-part MMA of a factor is skipped for the tiles
-// that carry none.  The tensor core's internal sums do not round to nearest, so
+// below FP32 rounding).  A factor column without a low part is itself only
+// BF16-accurate, so it meets X's and T's high parts alone: one MMA per tile
+// pair (phase 1 loads no X low part for units of such columns).  The tensor core's internal sums do not round to nearest, so
 // each short chain of MMAs goes into a zeroed temporary that is added to the
 // running FP32 sum with an ordinary FADD.
 #include <algorithm>
@@ -176,6 +177,7 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
   // the loop wait for nothing: lane 4j + t holds tile j's pair t
   int2 mm = make_int2(-1, -1);
   if (P.nchunk == 1 && lane < 4 * NCT && (lane >> 2) < u.nct) mm = tslot_pair(tslot, P.t0 + u.ct0 + (lane >> 2), lane);
+  const bool xlo = u.ct0 < P.nctl;  // the unit holds columns with low parts
   for (int r = 0; r < u.nrt; r += RU) {
     uint4 xf[RU][NH][4], vh[RU][NCT], vl[RU][NCT];
 #pragma unroll
@@ -186,7 +188,8 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
 #pragma unroll
       for (int h = 0; h < NH; ++h)
 #pragma unroll
-        for (int p = 0; p < 4; ++p) xf[q][h][p] = ok ? ld_keep(xp + h * xh + p * 32, keep) : z;
+        for (int p = 0; p < 4; ++p)  // X's low part only for units with low-part columns
+          xf[q][h][p] = ok && (p < 2 || xlo) ? ld_keep(xp + h * xh + p * 32, keep) : z;
       const uint4* hp = store + (P.hi1 + rt * P.nct + u.ct0) * 32 + lane;
       const uint4* lp = store + (P.lo1 + rt * P.nctl + u.ct0) * 32 + lane;
 #pragma unroll
@@ -204,9 +207,9 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
 #pragma unroll
             for (int h = 0; h < NH; ++h) {
               float d[4] = {0.f, 0.f, 0.f, 0.f};
-              mma_a4(d, xf[q][h][2], vh[q][j].x, vh[q][j].y);  // X_lo V_hi
-              mma_a4(d, xf[q][h][3], vh[q][j].z, vh[q][j].w);
-              if (u.ct0 + j < P.nctl) {                        // X_hi V_lo
+              if (u.ct0 + j < P.nctl) {  // a column with a low part: X_lo V_hi, X_hi V_lo
+                mma_a4(d, xf[q][h][2], vh[q][j].x, vh[q][j].y);
+                mma_a4(d, xf[q][h][3], vh[q][j].z, vh[q][j].w);
                 mma_a4(d, xf[q][h][0], vl[q][j].x, vl[q][j].y);
                 mma_a4(d, xf[q][h][1], vl[q][j].z, vl[q][j].w);
               }
@@ -377,13 +380,13 @@ __global__ void __launch_bounds__(32 * WARPS, 1) k_mx_p1r(const MxUnit* __restri
     // the column tiles' MMA chains interleaved, so that consecutive MMAs are independent
 #pragma unroll
     for (int j = 0; j < VT; ++j)
-      if (j < CU.nct) {
+      if (j < CU.nct && CU.ct0 + j < CP.nctl) {  // X_lo V_hi, for columns with low parts
         const uint4 vh = sl[(4 + j) * 32];
-        mma_a4(d[j], x2, vh.x, vh.y);  // X_lo V_hi
+        mma_a4(d[j], x2, vh.x, vh.y);
       }
 #pragma unroll
     for (int j = 0; j < VT; ++j)
-      if (j < CU.nct) {
+      if (j < CU.nct && CU.ct0 + j < CP.nctl) {
         const uint4 vh = sl[(4 + j) * 32];
         mma_a4(d[j], x3, vh.z, vh.w);
       }

@@ -447,6 +447,50 @@ def cg_solve(H, B, tol=1e-6, max_iter=1000, check_every=8, stream=None):
     return Xc.t(), it.value, res.value
 
 
+class PiecewiseHMatrix:
+    """An H-matrix kept out of device memory, in block-row pieces.
+
+    The rows are split into `pieces` runs of whole subtrees
+    (ranks.subtree_shards).  Each piece -- the blocks whose rows or columns
+    touch its rows (hm_hmatrix_build_rows) -- is built on the device, written
+    to a file in `directory` and freed, so the device never holds more than
+    one piece.  matvec() loads the pieces one at a time, multiplies all of X
+    and keeps each piece's rows.  A product costs `pieces` file reads and
+    panel rebuilds on top of the arithmetic: a way past the device's memory,
+    not a fast path.  (The reference's large-matrix variant treats its matrix
+    in p x p pieces; here a piece is a whole block row, whose blocks a product
+    needs together.)"""
+
+    def __init__(self, tree, structure, points, pieces, directory, stream=None, **build_kw):
+        import ranks
+
+        self.tree, self.structure, self.n = tree, structure, tree.n
+        self.shards = ranks.subtree_shards(tree.copy_out()["offsets"], pieces)
+        self.paths, self.piece_device_bytes = [], []
+        for i, (lb, le, r0, r1) in enumerate(self.shards):
+            H = build_hmatrix(tree, structure, points, leaves=(lb, le), stream=stream, **build_kw)
+            self.piece_device_bytes.append(H.stats()["device_bytes"])
+            path = os.path.join(str(directory), "piece_%d_of_%d.hmb" % (i, pieces))
+            H.save(path)
+            H.free()
+            self.paths.append(path)
+
+    def matvec(self, X, stream=None):
+        """Y = H X for a float32 CUDA tensor X (n, nrhs) (X.T contiguous), tree order."""
+        import torch
+
+        _check_vectors(X, self.n, "X")
+        nrhs = X.shape[1]
+        Y = torch.empty((nrhs, self.n), dtype=torch.float32, device=X.device).t()
+        Yp = torch.empty((nrhs, self.n), dtype=torch.float32, device=X.device).t()
+        for (lb, le, r0, r1), path in zip(self.shards, self.paths):
+            H = load_hmatrix(self.tree, self.structure, path, stream=stream)
+            H.matvec(X, Y=Yp, stream=stream)
+            Y[r0:r1] = Yp[r0:r1]
+            H.free()
+        return Y
+
+
 def load_hmatrix(tree, structure, path, stream=None):
     """Read an H-matrix written by HMatrix.save (hm_hmatrix_load); tree and
     structure must be the ones it was built on."""

@@ -227,10 +227,21 @@ def test_mixed_form_holds_no_fp32_factors(hm):
     kind, ell, nugget, tol = hm.K_MATERN32, 0.2, 1e-3, 1e-4
     pts, tree, st, Hm = build(hm, n, d, b, kind, ell, tol, 128, nugget=nugget, seed=11, precision=hm.PREC_MIXED)
     s = Hm.stats()
-    # beyond the panels only the product's workspaces remain (projection
-    # scratch for 128 right-hand sides, the per-pass X and Y copies): less than
-    # the FP32 factors alone would take
-    assert s["device_bytes"] - s["mixed_bytes"] < s["factor_bytes"], s
+    # beyond the panels only the product's plan and workspaces remain: per
+    # 16-column part of a 128-column pass (8 parts), X fragments (512 floats
+    # per 32-row tile), projections (at most 16 words per factor column) and
+    # chunk partials; the per-pass X and Y copies (2 x 128 floats per point);
+    # the block lists.  The FP32 factors and dense blocks are not held.
+    # (panel padding: at most 7 columns, 128 words, per panel, at most two
+    # panels per leaf)
+    nleaf = 1 << tree.depth
+    tiles = n // 32 + nleaf
+    scratch = 8 * 4 * (512 * tiles + 16 * s["rank_sum"] + 128 * 2 * nleaf) + (1 << 20)
+    lists = 8 * 128 * n + 200 * (s["num_lowrank"] + s["num_dense"])
+    held = s["device_bytes"] - s["mixed_bytes"]
+    assert held < scratch + lists, s
+    # the bound is tight enough to see FP32 factors, had they been kept
+    assert scratch + lists < held + s["factor_bytes"] + s["dense_bytes"], s
     # a dense block read back is the kernel to BF16 hi + lo accuracy
     _, dense = Hm.blocks()
     perm = tree.copy_out()["perm"]

@@ -83,3 +83,25 @@ def test_fp64_vectors_match_fp32_product(hm, cloud):
                                     X.t().cpu().numpy()).T
     err = np.linalg.norm(Y64.cpu().numpy()[rows] - Yref) / np.linalg.norm(Yref)
     assert err < 1e-5, err
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_piecewise_out_of_core_product(hm, cloud, prec, tmp_path):
+    """The out-of-core form: the matrix built as three block-row pieces, each
+    written to a file and freed; the product loads one piece at a time.  It
+    equals the in-memory product, and no piece needs the whole matrix's
+    device memory."""
+    import torch
+
+    n, d, pts, tree, st = cloud
+    kw = dict(kernel=hm.K_MATERN32, ell=0.2, nugget=1e-3, tol=1e-5, max_rank=128, precision=prec, seed=3)
+    H = hm.build_hmatrix(tree, st, pts, **kw)
+    X = torch.randn((7, n), device="cuda").t()
+    Y = H.matvec(X)
+    whole = H.stats()["device_bytes"]
+    del H
+    P = hm.PiecewiseHMatrix(tree, st, pts, 3, tmp_path, **kw)
+    assert max(P.piece_device_bytes) < whole
+    Yp = P.matvec(X)
+    rel = (torch.linalg.norm(Yp - Y) / torch.linalg.norm(Y)).item()
+    assert rel < 1e-6, rel
