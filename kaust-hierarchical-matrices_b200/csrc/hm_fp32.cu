@@ -241,7 +241,7 @@ __device__ __forceinline__ void fp_p2_step(float (&acc)[2][2][4], const uint32_t
 // One warp per global row tile (32 rows of one leaf), as the mixed form's
 // phase 2: every ancestor cluster's panel rows times its T, then the dense
 // blocks of the leaf row.
-__global__ void __launch_bounds__(32, 20) k_fp_p2(int tile0, int tile_end, int depth,
+__global__ void __launch_bounds__(32, 24) k_fp_p2(int tile0, int tile_end, int depth,
                                                   const int* __restrict__ tile_leaf,
                                                   const int* __restrict__ leaf_tile0,
                                                   const int* __restrict__ leaf_off, const int* __restrict__ pan_of,

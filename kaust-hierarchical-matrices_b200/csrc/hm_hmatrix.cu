@@ -1397,10 +1397,11 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       for (int round = 0; round < max_rounds; ++round) {
         if (fast) {
           // basis + test columns: double width in the first round and again
-          // from the third on (the blocks still active by then are the
+          // from the fourth on (the blocks still active by then are the
           // high-rank ones; entry generation, not the sample width, is the
-          // cost of a round, so wider rounds mean fewer of them)
-          const int rbs = (round == 1 ? bs : bs0) + bst;
+          // cost of a round, so wider rounds mean fewer of them; earlier, a
+          // wider basis would cost more in the projection than it saves)
+          const int rbs = (round == 1 || round == 2 ? bs : bs0) + bst;
           k_omega_pack<<<592, 256, 0, stream>>>(om2.p, om_rows2 / 8, rbs, bs8 / 8, ka.seed, round);
           HM_LAUNCH_CHECK();
           kf.round = round;
