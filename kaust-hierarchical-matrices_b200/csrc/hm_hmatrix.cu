@@ -529,17 +529,21 @@ struct OrthArgs {
   int round;
 };
 
-// C[j][c] = sum_i Q[i, j] Y[i, c]  (k x bs), result in shared Csm
-template <typename W>
-__device__ void block_qty(const W* Q, const W* Y, int m, int k, int bs, W* Csm, W* stage) {
+// C[j][c] = sum_i Q[i, j] Y[i, c]  (k x bs), result in shared Csm.  Each
+// thread owns a TA x 4 tile of C (rows j = 8 * TA-blocks, columns c in fours),
+// so that a staged value serves TA or 4 FMAs instead of one; TA grows with k
+// so that the 256 threads stay busy.  Every output sums its products in the
+// same order (rows of a 32-row chunk in turn, chunks in turn) for any TA.
+template <typename W, int TA>
+__device__ void block_qty_t(const W* Q, const W* Y, int m, int k, int bs, W* Csm, W* stage) {
   const int t = threadIdx.x;
-  constexpr int kPer = kMaxCols * max_bs<W>() / kOrthThreads;  // outputs per thread
-  W accv[kPer];
+  const int jg = t >> 3, cg = t & 7;  // 32 row groups of TA x 8 column groups of 4
+  W acc[TA][4];
 #pragma unroll
-  for (int i = 0; i < kPer; ++i) accv[i] = W(0);
+  for (int a = 0; a < TA; ++a) acc[a][0] = acc[a][1] = acc[a][2] = acc[a][3] = W(0);
   W* Qs = stage;                  // [kMaxCols][33]
   W* Ys = stage + kMaxCols * 33;  // [max_bs][33]
-  const int nout = k * bs;
+  const bool act = jg * TA < k && cg * 4 < bs;
   for (int i0 = 0; i0 < m; i0 += 32) {
     for (int e = t; e < 32 * k; e += kOrthThreads) {
       int ii = e & 31, j = e >> 5;
@@ -550,24 +554,43 @@ __device__ void block_qty(const W* Q, const W* Y, int m, int k, int bs, W* Csm, 
       Ys[c * 33 + ii] = (i0 + ii < m) ? Y[(size_t)c * m + i0 + ii] : W(0);
     }
     __syncthreads();
+    if (act) {
+      for (int ii = 0; ii < 32; ++ii) {
+        W q[TA], y[4];
 #pragma unroll
-    for (int x = 0; x < kPer; ++x) {
-      int o = t + x * kOrthThreads;
-      if (o < nout) {
-        int j = o / bs, c = o % bs;
-        W sacc = accv[x];
-        for (int ii = 0; ii < 32; ++ii) sacc = fma(Qs[j * 33 + ii], Ys[c * 33 + ii], sacc);
-        accv[x] = sacc;
+        for (int a = 0; a < TA; ++a) q[a] = Qs[(jg * TA + a) * 33 + ii];  // rows j >= k: never stored
+#pragma unroll
+        for (int b = 0; b < 4; ++b) y[b] = Ys[(cg * 4 + b) * 33 + ii];
+#pragma unroll
+        for (int a = 0; a < TA; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] = fma(q[a], y[b], acc[a][b]);
       }
     }
     __syncthreads();
   }
+  if (act) {
 #pragma unroll
-  for (int x = 0; x < kPer; ++x) {
-    int o = t + x * kOrthThreads;
-    if (o < nout) Csm[o] = accv[x];  // Csm[j*bs + c]
+    for (int a = 0; a < TA; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int j = jg * TA + a, c = cg * 4 + b;
+        if (j < k && c < bs) Csm[j * bs + c] = acc[a][b];
+      }
   }
   __syncthreads();
+}
+
+template <typename W>
+__device__ void block_qty(const W* Q, const W* Y, int m, int k, int bs, W* Csm, W* stage) {
+  if (k <= 32)
+    block_qty_t<W, 1>(Q, Y, m, k, bs, Csm, stage);
+  else if (k <= 64)
+    block_qty_t<W, 2>(Q, Y, m, k, bs, Csm, stage);
+  else if (k <= 128)
+    block_qty_t<W, 4>(Q, Y, m, k, bs, Csm, stage);
+  else
+    block_qty_t<W, 8>(Q, Y, m, k, bs, Csm, stage);
 }
 
 // Y -= Q C
@@ -585,38 +608,47 @@ __device__ void block_update(const W* Q, W* Y, int m, int k, int bs, const W* Cs
   __syncthreads();
 }
 
-// G = Y^T Y in FP64 (cols x cols), into shared Gs
+// G = Y^T Y in FP64 (cols x cols), into shared Gs.  Each thread owns a 2 x 2
+// tile of the upper triangle (the lower one is its mirror: a product of two
+// values is the same in either order), so a staged value serves two
+// products; every entry sums its products in row order.
 template <typename W>
 __device__ void gram64(const W* Y, int m, int cols, double* Gs, W* stage) {
+  static_assert(max_bs<W>() <= 32, "2 x 2 tiles of 16 x 16 threads cover 32 columns");
   const int t = threadIdx.x;
-  constexpr int kPer = max_bs<W>() * max_bs<W>() / kOrthThreads;  // outputs per thread
-  double accv[kPer];
-#pragma unroll
-  for (int x = 0; x < kPer; ++x) accv[x] = 0.0;
+  const int ta = t >> 4, tb = t & 15;  // rows 2 ta, 2 ta + 1; columns 2 tb, 2 tb + 1
+  const bool act = ta <= tb && 2 * tb < cols;
+  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
   W* Ys = stage;  // [max_bs][33]
-  const int nout = cols * cols;
   for (int i0 = 0; i0 < m; i0 += 32) {
     for (int e = t; e < 32 * cols; e += kOrthThreads) {
       int ii = e & 31, c = e >> 5;
       Ys[c * 33 + ii] = (i0 + ii < m) ? Y[(size_t)c * m + i0 + ii] : W(0);
     }
     __syncthreads();
-#pragma unroll
-    for (int x = 0; x < kPer; ++x) {
-      int o = t + x * kOrthThreads;
-      if (o < nout) {
-        int a = o / cols, b = o % cols;
-        double sacc = accv[x];
-        for (int ii = 0; ii < 32; ++ii) sacc += (double)Ys[a * 33 + ii] * (double)Ys[b * 33 + ii];
-        accv[x] = sacc;
+    if (act) {
+      for (int ii = 0; ii < 32; ++ii) {
+        const double y0 = (double)Ys[(2 * ta) * 33 + ii], y1 = (double)Ys[(2 * ta + 1) * 33 + ii];
+        const double z0 = (double)Ys[(2 * tb) * 33 + ii], z1 = (double)Ys[(2 * tb + 1) * 33 + ii];
+        acc[0][0] += y0 * z0;
+        acc[0][1] += y0 * z1;
+        acc[1][0] += y1 * z0;
+        acc[1][1] += y1 * z1;
       }
     }
     __syncthreads();
   }
+  if (act) {
 #pragma unroll
-  for (int x = 0; x < kPer; ++x) {
-    int o = t + x * kOrthThreads;
-    if (o < nout) Gs[o] = accv[x];
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        const int a = 2 * ta + u, b = 2 * tb + v;
+        if (a < cols && b < cols) {
+          Gs[a * cols + b] = acc[u][v];
+          Gs[b * cols + a] = acc[u][v];
+        }
+      }
   }
   __syncthreads();
 }
