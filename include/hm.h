@@ -184,6 +184,12 @@ typedef struct {
   unsigned long long seed;  /* seed of the Gaussian test matrices */
   int diag_from_coords;     /* diagonal leaf blocks: 0 stored, 1 recomputed from the coordinates in
                                every product, -1 (default) recomputed for derivative builds only */
+  int level_schedule;       /* 0 (default): tol and max_rank at every level above the leaves;
+                               1: the reference's schedule -- the tolerance doubles at each level
+                               above the leaves (tol 2^(depth - l) at level l,
+                               src/constructHMatrixFromStruct.cu:31,54) and the cap at level l is
+                               bucket 2^i, / 4 beyond i = 5, i = depth - 1 - l (generateMaxRanks,
+                               src/helperFunctions.cu:67-74), at most 256; max_rank is unused */
 } hm_build_opts;
 
 /* Fills opts with the reference's settings: exp kernel, l = 0.2 if d == 3

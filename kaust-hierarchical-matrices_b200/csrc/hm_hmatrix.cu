@@ -62,6 +62,7 @@ struct Prob {
   int level;
   int u, v;
   long long qoff, yoff, boff;  // workspace offsets (floats)
+  double tscale2;              // (this block's tolerance / the build's)^2: 1, or the level schedule's
 };
 
 struct ProbState {
@@ -797,7 +798,7 @@ __global__ void __launch_bounds__(kOrthThreads) k_orth(OrthArgs<W> a) {
       const double est = tr / ne;
       S.est = est;
       S.rounds += 1;
-      if (est <= a.thresh2 * S.normA2 || S.normA2 == 0.0) decision = 1;
+      if (est <= a.thresh2 * P.tscale2 * S.normA2 || S.normA2 == 0.0) decision = 1;
       else if (k + bsb > P.kmax) decision = 2;
       else decision = 0;
     }
@@ -827,7 +828,7 @@ __global__ void __launch_bounds__(kOrthThreads) k_orth(OrthArgs<W> a) {
     }
     const double tr = trace_gram(Yt, m, bst, Gs, stage);
     if (threadIdx.x == 0) S.est = tr / bst;
-    conv = tr / bst <= a.thresh2 * S.normA2;
+    conv = tr / bst <= a.thresh2 * P.tscale2 * S.normA2;
     if (!conv && k < P.kmax) {
       int rt = cholqr_block(Q, k, Yt, m, bst, Gs, perm, &rank_sh, Csm, stage);
       rt = min(rt, P.kmax - k);
@@ -1025,7 +1026,8 @@ __global__ void __launch_bounds__(kGramThreads) k_jacobi(const Prob* probs, Prob
   __shared__ int r_sh;
   if (t == 0) {
     // discard the smallest eigenvalues while their sum fits the budget
-    double budget = tol2 * S.normA2 - S.est;
+    const double ts2 = probs[p].tscale2;
+    double budget = tol2 * ts2 * S.normA2 - S.est;
     double tail = 0;
     int r = k;
     if (S.converged && budget > 0) {
@@ -1047,7 +1049,7 @@ __global__ void __launch_bounds__(kGramThreads) k_jacobi(const Prob* probs, Prob
       const double c = 2.0 * 0x1p-18;  // (2^-9)^2 for each of u_j and v_j
       while (rhi > 0) {
         double l = fmax(G[order[rhi - 1] * kp + order[rhi - 1]], 0.0);
-        if (rt + c * l > rbudget * S.normA2) break;
+        if (rt + c * l > rbudget * ts2 * S.normA2) break;
         rt += c * l;
         --rhi;
       }
@@ -1190,6 +1192,8 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   const int bs = opt.sample_block;
   if (opt.max_rank > kMaxCols || opt.leaf_max_rank > kMaxCols)
     return fail(HM_ERR_UNSUPPORTED, "hm_hmatrix_build: rank caps must be <= 256");
+  if (opt.level_schedule != 0 && opt.level_schedule != 1)
+    return fail(HM_ERR_INVALID, "hm_hmatrix_build: level_schedule must be 0 or 1");
 
   cudaEvent_t ev0, ev1;
   HM_CUDA(cudaEventCreate(&ev0));
@@ -1219,6 +1223,26 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
   const int depth = t->depth;
   const std::vector<int>& lo = t->h_offsets;
   auto coff = [&](int level, int c) { return lo[(size_t)c << (depth - level)]; };
+  // Rank cap and tolerance of a level-l block.  Uniform: the leaf cap at the
+  // leaf level, max_rank above it, tol everywhere.  The reference's schedule
+  // (level_schedule = 1): the tolerance doubles at each level above the
+  // leaves (src/constructHMatrixFromStruct.cu:31,54: tol 2^(depth - l) at
+  // level l) and the cap is bucket 2^i, divided by 4 beyond i = 5, with
+  // i = depth - 1 - l (generateMaxRanks, src/helperFunctions.cu:67-74),
+  // within this build's largest basis.
+  auto level_cap = [&](int l) {
+    if (l == depth) return opt.leaf_max_rank;
+    if (opt.level_schedule != 1) return opt.max_rank;
+    const int i = depth - 1 - l;
+    long long c = (long long)t->bucket << std::min(i, 20);
+    if (i > 5) c /= 4;
+    return (int)std::min<long long>(c, kMaxCols);
+  };
+  auto level_tscale2 = [&](int l) {
+    if (opt.level_schedule != 1 || l >= depth) return 1.0;
+    const double f = std::ldexp(1.0, depth - l);
+    return f * f;
+  };
   // rows of the shard; a pair is needed when its rows or its columns overlap them
   const int row_lo = lo[leaf_lo], row_hi = lo[leaf_hi];
   auto needed = [&](int r0, int m, int c0, int n) {
@@ -1244,7 +1268,8 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
       P.m = coff(l, v + 1) - P.r0;
       P.c0 = coff(l, u);
       P.n = coff(l, u + 1) - P.c0;
-      P.kmax = std::min(l == depth ? opt.leaf_max_rank : opt.max_rank, std::min(P.m, P.n));
+      P.kmax = std::min(level_cap(l), std::min(P.m, P.n));
+      P.tscale2 = level_tscale2(l);
       if (!needed(P.r0, P.m, P.c0, P.n)) continue;
       probs.push_back(P);
     }
@@ -1591,7 +1616,8 @@ hm_status hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, con
               C.c0 = coff(cl, C.u);
               C.n = coff(cl, C.u + 1) - C.c0;
               if (C.m <= 0 || C.n <= 0 || !needed(C.r0, C.m, C.c0, C.n)) continue;
-              C.kmax = std::min(cl == depth ? opt.leaf_max_rank : opt.max_rank, std::min(C.m, C.n));
+              C.kmax = std::min(level_cap(cl), std::min(C.m, C.n));
+              C.tscale2 = level_tscale2(cl);
               children.push_back(C);
             }
           continue;
@@ -1834,6 +1860,7 @@ void hm_build_opts_default(int d, hm_build_opts* o) {
   o->derivative = 0;
   o->seed = 0;
   o->diag_from_coords = -1;
+  o->level_schedule = 0;
 }
 
 hm_status hm_hmatrix_build(hm_kdtree t, hm_structure s, const double* d_points, const hm_build_opts* opts,

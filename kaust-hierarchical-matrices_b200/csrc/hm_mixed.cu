@@ -243,6 +243,65 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
   }
 }
 
+// A unit whose columns have no low parts: X's and V's high parts only, one
+// MMA per tile pair (the same sums as mx_p1_unit takes for such columns).
+// Without the low parts' registers a warp keeps RU row tiles of loads in
+// flight instead of two.
+template <int NCT, int RU>
+__device__ __forceinline__ void mx_p1_unit_hi(const MxUnit& u, const MxPanel& P, const uint4* __restrict__ store,
+                                              const uint4* __restrict__ Xf, const int* __restrict__ tslot,
+                                              float4* __restrict__ S, uint32_t* __restrict__ T, int lane) {
+  float acc[NCT][4];
+#pragma unroll
+  for (int j = 0; j < NCT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+  const uint64_t keep = l2_keep_policy();
+  int2 mm = make_int2(-1, -1);
+  if (P.nchunk == 1 && lane < 4 * NCT && (lane >> 2) < u.nct) mm = tslot_pair(tslot, P.t0 + u.ct0 + (lane >> 2), lane);
+  for (int r = 0; r < u.nrt; r += RU) {
+    uint4 xf[RU][2], vh[RU][NCT];
+#pragma unroll
+    for (int q = 0; q < RU; ++q) {
+      const bool ok = r + q < u.nrt;
+      const long long rt = u.rt0 + r + q;
+      const uint4* xp = Xf + (size_t)(P.tile0 + rt) * 128 + lane;
+      xf[q][0] = ok ? ld_keep(xp, keep) : z;
+      xf[q][1] = ok ? ld_keep(xp + 32, keep) : z;
+      const uint4* hp = store + (P.hi1 + rt * P.nct + u.ct0) * 32 + lane;
+#pragma unroll
+      for (int j = 0; j < NCT; ++j) vh[q][j] = ok && j < u.nct ? __ldcs(hp + j * 32) : z;
+    }
+#pragma unroll
+    for (int q = 0; q < RU; ++q) {
+      if (r + q < u.nrt) {
+#pragma unroll
+        for (int j = 0; j < NCT; ++j) {
+          if (j < u.nct) {
+            float d[4] = {0.f, 0.f, 0.f, 0.f};
+            mma_a4(d, xf[q][0], vh[q][j].x, vh[q][j].y);  // X_hi V_hi
+            mma_a4(d, xf[q][1], vh[q][j].z, vh[q][j].w);
+            add4(acc[j], d);
+          }
+        }
+      }
+    }
+  }
+  if (P.nchunk == 1) {
+#pragma unroll
+    for (int j = 0; j < NCT; ++j)
+      if (j < u.nct) {
+        const int src = 4 * j + (lane & 3);
+        const int2 m = make_int2(__shfl_sync(0xffffffffu, mm.x, src), __shfl_sync(0xffffffffu, mm.y, src));
+        mx_store_t(T, m, lane, acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+      }
+  } else {
+    float4* out = S + (P.s0 + (long long)u.chunk * P.nct + u.ct0) * 32 + lane;
+#pragma unroll
+    for (int j = 0; j < NCT; ++j)
+      if (j < u.nct) out[j * 32] = make_float4(acc[j][0], acc[j][1], acc[j][2], acc[j][3]);
+  }
+}
+
 // One unit per CTA.  WPC = 1: one warp per CTA, 16 per SM (measured): a warp
 // runs one unit and retires at once, instead of holding its CTA's slot until
 // sibling warps with other units finish; 16 warps keep enough loads in flight
@@ -268,7 +327,14 @@ __global__ void __launch_bounds__(32 * WPC, kP1PerSm / WPC) k_mx_p1(const MxUnit
   }
   const MxUnit u = units[w];
   const MxPanel P = panels[u.panel];
-  if (NH == 1) {
+  if (NH == 1 && u.ct0 >= P.nctl) {  // no low parts in this unit
+    if (u.nct > 4)
+      mx_p1_unit_hi<8, 2>(u, P, store, Xf, tslot, S, T, lane);
+    else if (u.nct > 2)
+      mx_p1_unit_hi<4, 4>(u, P, store, Xf, tslot, S, T, lane);
+    else
+      mx_p1_unit_hi<2, 6>(u, P, store, Xf, tslot, S, T, lane);
+  } else if (NH == 1) {
     if (u.nct > 4)
       mx_p1_unit<8, 1, 1>(u, P, store, Xf, tslot, S, T, xh, sh, th, lane);
     else if (u.nct > 2)

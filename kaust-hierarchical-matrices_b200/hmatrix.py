@@ -48,6 +48,7 @@ class BuildOpts(ctypes.Structure):
         ("derivative", ctypes.c_int),
         ("seed", ctypes.c_ulonglong),
         ("diag_from_coords", ctypes.c_int),
+        ("level_schedule", ctypes.c_int),
     ]
 
 
@@ -512,7 +513,7 @@ def default_opts(d):
 
 def build_hmatrix(tree, structure, points=None, kernel=K_EXP, ell=None, nugget=0.0, tol=1e-5, max_rank=64,
                   leaf_max_rank=0, sample_block=16, precision=PREC_FP32, derivative=0, seed=0, stream=None,
-                  diag_from_coords=-1, leaves=None):
+                  diag_from_coords=-1, leaves=None, level_schedule=0):
     """hm_hmatrix_build; with leaves=(leaf_begin, leaf_end), the block-row
     shard of those leaves' rows (hm_hmatrix_build_rows)."""
     o = default_opts(tree.d)
@@ -528,6 +529,7 @@ def build_hmatrix(tree, structure, points=None, kernel=K_EXP, ell=None, nugget=0
     o.derivative = derivative
     o.seed = seed
     o.diag_from_coords = diag_from_coords
+    o.level_schedule = level_schedule
     h = ctypes.c_void_p()
     pp = _ptr(points) if points is not None else None
     if leaves is None:

@@ -314,3 +314,45 @@ def test_mixed_two_half_passes_match_single_passes(hm, diag_from_coords):
             Ys = torch.cat(parts, dim=1)
             scale = torch.linalg.norm(Ys).item()
             assert torch.linalg.norm(Y - Ys).item() <= 1e-6 * scale, (ncol, orig)
+
+
+def test_reference_level_schedule(hm):
+    """level_schedule = 1: the reference's compression schedule -- the
+    tolerance doubles at each level above the leaves
+    (src/constructHMatrixFromStruct.cu:31,54) and the rank cap at level l is
+    bucket 2^i, / 4 beyond i = 5, i = depth - 1 - l (generateMaxRanks,
+    src/helperFunctions.cu:67-74).  Every block meets its own level's
+    tolerance and cap, coarser levels end with lower ranks than under one
+    tolerance, and the product stays within the coarsest tolerance."""
+    n, d, b = 8192, 2, 32
+    kind, ell, tol = hm.K_EXP, 0.1, 1e-6
+    pts = hm.generate_dataset(n, d, seed=1234)
+    tree = hm.construct_kdtree(pts, n, d, b)
+    st = hm.construct_hmatrix_structure(tree, hm.BOX_CENTER, 1.0)
+    H = hm.build_hmatrix(tree, st, pts, kernel=kind, ell=ell, tol=tol, max_rank=64, level_schedule=1)
+    Hu = hm.build_hmatrix(tree, st, pts, kernel=kind, ell=ell, tol=tol, max_rank=64)
+    depth = tree.depth
+    lr, _ = H.blocks()
+    lru, _ = Hu.blocks()
+    ph = pts.cpu().numpy()
+    perm = tree.copy_out()["perm"]
+    rng = np.random.default_rng(4)
+    idx = np.nonzero(lr[:, 0] > lr[:, 2])[0]
+    for i in rng.choice(idx, min(len(idx), 150), replace=False):
+        r0, m, c0, nn, k, lvl = (int(x) for x in lr[i])
+        if lvl < depth:
+            i_ = depth - 1 - lvl
+            cap = min(256, (b << i_) // (4 if i_ > 5 else 1))
+            assert k <= cap, (lvl, k, cap)
+        U, V = H.block_factors(int(i))
+        err = oracle.block_error(ph, n, d, perm, kind, ell, 0.0, r0, m, c0, nn, U, V)
+        assert err <= tol * 2 ** (depth - lvl), (lvl, err)
+    top = lr[:, 5] <= depth - 3
+    assert lr[top, 4].sum() < lru[lru[:, 5] <= depth - 3, 4].sum()
+    import torch
+
+    X = torch.randn((n, 2), device="cuda")
+    Y = H.matvec(X).cpu().numpy()
+    rows = rng.choice(n, 300, replace=False)
+    Yref = oracle.dense_rows_matvec(ph, n, d, perm, kind, ell, 0.0, rows, X.t().cpu().numpy().astype(np.float64)).T
+    assert np.linalg.norm(Y[rows] - Yref) / np.linalg.norm(Yref) < tol * 2 ** (depth - 1)
