@@ -427,6 +427,8 @@ def run_ours(args):
                                                     precision=prec, seed=7, stream=stream,
                                                     leaves=own[:2] if sharded else None))
         build_s[f] = front_s + t
+        if f == "mixed" and args.schedule:
+            hm.schedule_set(Hs[f], args.schedule, stream=stream)
     head = forms[0]
 
     gen = torch.Generator(device=dev)
@@ -471,6 +473,7 @@ def run_ours(args):
         nr = min(width, nrhs)
         panels = (nrhs + width - 1) // width
         ms = timed(step_of(Hs[f]), clocks if f == head else None)
+        Hs[f].check()  # no bounded device-side wait gave up in the timed products
         kt = kernel_times(hm, lib, Hs[f], X, Y, n, nr, stream)
         bp, be = ctypes.c_longlong(), ctypes.c_longlong()
         mp, me = ctypes.c_float(), ctypes.c_float()
@@ -830,6 +833,9 @@ def main():
                          "job's clouds spread over the ranks)")
     ap.add_argument("--check-rows", type=int, default=4096,
                     help="rows of the FP64 oracle's dense product the error is measured on")
+    ap.add_argument("--schedule", default=None,
+                    help="mixed form: a schedule in hm_autotune's notation, e.g. "
+                         "'mixed chunk_tiles=128 group_tiles=4 p1_ring=0 wide_tc=0'")
     ap.add_argument("--skip-check", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)

@@ -386,6 +386,13 @@ HM_API void hm_hmatrix_free(hm_hmatrix h);
 HM_API hm_status hm_hmatrix_save(hm_hmatrix h, const char* path);
 HM_API hm_status hm_hmatrix_load(hm_kdtree t, hm_structure s, const char* path, void* stream, hm_hmatrix* out);
 
+/* Waits for the stream, then returns HM_ERR_TIMEOUT if a bounded device-side
+ * wait in one of this matrix's product kernels gave up since the last check
+ * (the products concerned hold wrong values; the report is cleared), else
+ * HM_OK.  Only the tcgen05 phase 1 of the mixed form's 128-column passes
+ * waits on the device; the wait ends the kernel instead of hanging it. */
+HM_API hm_status hm_hmatrix_check(hm_hmatrix h, void* stream);
+
 /* Schedule autotuner (no counterpart in the reference).  Times the product's
  * schedule candidates on this matrix (nrhs columns, at most one pass of the
  * product: 128 for the mixed form, 16 for the FP32 form) and keeps the
@@ -402,9 +409,12 @@ HM_API hm_status hm_autotune(hm_hmatrix h, int nrhs, const char* cache_path, voi
                              char* choice, int choice_len);
 
 /* Applies a schedule given as hm_autotune describes it, e.g.
- * "mixed chunk_tiles=64 group_tiles=8 p1_ring=1", "fp32 chunk_tiles=32
+ * "mixed chunk_tiles=64 group_tiles=8 p1_ring=1 wide_tc=1", "fp32 chunk_tiles=32
  * group_tiles=4" (FP32 panels) or "fp32 p1_rows=256" (FP32 per-block
- * kernels; they read the FP32 factors, which FP32 matrices keep). */
+ * kernels; they read the FP32 factors, which FP32 matrices keep).  For the
+ * mixed form, wide_tc (optional; 0 by default) selects tcgen05 kernels for
+ * both phases of passes of 65-128 right-hand sides (0: the warp-level MMA
+ * kernels, the faster of the two as measured). */
 HM_API hm_status hm_schedule_set(hm_hmatrix h, const char* choice, void* stream);
 
 /* --- Batches of independent clouds ------------------------------------------

@@ -29,6 +29,7 @@ namespace {
 // group tiles >= 1, 0); FP32 per-block kernels: (p1 rows, 0, 0)
 struct Choice {
   int a = 0, b = 0, c = 0;
+  int d = -1;  // mixed: tcgen05 phase 1 for 128-column passes (1 on, 0 off, -1 unchanged)
 };
 
 bool is_mixed(hm_hmatrix h) { return h->opts.precision == HM_PREC_MIXED; }
@@ -36,7 +37,8 @@ bool is_mixed(hm_hmatrix h) { return h->opts.precision == HM_PREC_MIXED; }
 std::string describe(hm_hmatrix h, const Choice& c) {
   char buf[96];
   if (is_mixed(h))
-    std::snprintf(buf, sizeof buf, "mixed chunk_tiles=%d group_tiles=%d p1_ring=%d", c.a, c.b, c.c);
+    std::snprintf(buf, sizeof buf, "mixed chunk_tiles=%d group_tiles=%d p1_ring=%d wide_tc=%d", c.a, c.b, c.c,
+                  c.d >= 0 ? c.d : (h->mx.wide_tc ? 1 : 0));
   else if (c.b > 0)
     std::snprintf(buf, sizeof buf, "fp32 chunk_tiles=%d group_tiles=%d", c.a, c.b);
   else
@@ -47,6 +49,7 @@ std::string describe(hm_hmatrix h, const Choice& c) {
 hm_status apply(hm_hmatrix h, const Choice& c, cudaStream_t s) {
   if (is_mixed(h) || c.b > 0) {
     h->mx.enabled = true;
+    if (c.d >= 0) h->mx.wide_tc = c.d != 0;
     HM_TRY(mixed_schedule(h, c.a, c.b, c.c, s));
   } else {
     h->mx.enabled = false;  // the FP32 per-block kernels
@@ -162,7 +165,9 @@ extern "C" hm_status hm_schedule_set(hm_hmatrix h, const char* choice, void* str
   if (!h || !choice) return fail(HM_ERR_INVALID, "hm_schedule_set: null argument");
   Choice c;
   if (is_mixed(h)) {
-    if (std::sscanf(choice, "mixed chunk_tiles=%d group_tiles=%d p1_ring=%d", &c.a, &c.b, &c.c) != 3)
+    const int got = std::sscanf(choice, "mixed chunk_tiles=%d group_tiles=%d p1_ring=%d wide_tc=%d", &c.a, &c.b,
+                                &c.c, &c.d);
+    if (got < 3 || (got == 4 && c.d != 0 && c.d != 1))
       return fail(HM_ERR_INVALID, std::string("hm_schedule_set: not a mixed-form schedule: ") + choice);
   } else if (std::sscanf(choice, "fp32 chunk_tiles=%d group_tiles=%d", &c.a, &c.b) == 2) {
     if (c.b < 1 || c.b > 8)

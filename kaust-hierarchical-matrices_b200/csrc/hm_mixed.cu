@@ -123,10 +123,15 @@ __device__ __forceinline__ int2 tslot_pair(const int* __restrict__ tslot, long l
 // Xf[tile][part][lane], part 0/1 = hi of rows 0-15 / 16-31, part 2/3 = lo:
 // the m16n8k16 A fragment of X^T (16 right-hand sides x 16 rows):
 //   {X[2t,2t+1][g], X[2t,2t+1][g+8], X[2t+8,2t+9][g], X[2t+8,2t+9][g+8]}
+// Xtc (a 128-column pass on tcgen05, else null): per tile a 16 KB image,
+// hi then lo, of B = X in the K-major core-matrix layout, right-hand side n
+// and K block c (8 rows, in the order rho(c, e) = 8 (e / 2) + 2 c + e % 2 of
+// the factors' P1 lanes) at 16 bytes (n % 8) + 128 (n / 8) + 2048 c.
 __global__ void __launch_bounds__(128) k_mx_split_x(const float* __restrict__ X, int ldx, int nr, int num_tiles,
                                                     const int* __restrict__ tile_leaf,
                                                     const int* __restrict__ leaf_tile0,
-                                                    const int* __restrict__ leaf_off, uint4* __restrict__ Xf) {
+                                                    const int* __restrict__ leaf_off, uint4* __restrict__ Xf,
+                                                    uint4* __restrict__ Xtc) {
   __shared__ float xs[4][16][33];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int G = blockIdx.x * 4 + w;
@@ -141,6 +146,21 @@ __global__ void __launch_bounds__(128) k_mx_split_x(const float* __restrict__ X,
 #pragma unroll
   for (int r = 0; r < 16; ++r) xs[w][r][lane] = (ok && r < nr) ? __ldg(X + (size_t)r * ldx + row) : 0.f;
   __syncwarp();
+  if (Xtc) {  // this part's 16 right-hand sides x 4 K blocks (no fragments)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int idx = lane + 32 * q, nl = idx >> 2, c = idx & 3;
+      uint32_t hi[4], lo[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e)  // rows rho(c, 2e), rho(c, 2e + 1) = 8 e + 2 c + {0, 1}
+        split_bf16x2(xs[w][nl][8 * e + 2 * c], xs[w][nl][8 * e + 2 * c + 1], hi[e], lo[e]);
+      const int n = 16 * blockIdx.y + nl;
+      uint4* dst = Xtc + (size_t)G * 1024 + (n & 7) + (n >> 3) * 8 + c * 128;
+      dst[0] = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+      dst[512] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    }
+    return;
+  }
   const int g = lane >> 2, t = lane & 3;
 #pragma unroll
   for (int s = 0; s < 2; ++s) {
@@ -244,9 +264,8 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
 }
 
 // A unit whose columns have no low parts: X's and V's high parts only, one
-// MMA per tile pair (the same sums as mx_p1_unit takes for such columns).
-// Without the low parts' registers a warp keeps RU row tiles of loads in
-// flight instead of two.
+// MMA per tile pair.  Without the low parts' registers a warp keeps RU row
+// tiles of loads in flight instead of two.
 template <int NCT, int RU>
 __device__ __forceinline__ void mx_p1_unit_hi(const MxUnit& u, const MxPanel& P, const uint4* __restrict__ store,
                                               const uint4* __restrict__ Xf, const int* __restrict__ tslot,
@@ -271,18 +290,18 @@ __device__ __forceinline__ void mx_p1_unit_hi(const MxUnit& u, const MxPanel& P,
 #pragma unroll
       for (int j = 0; j < NCT; ++j) vh[q][j] = ok && j < u.nct ? __ldcs(hp + j * 32) : z;
     }
+    // one chain over the step's row tiles per column tile (BF16-accurate
+    // products: the chain's drift is far below their rounding)
 #pragma unroll
-    for (int q = 0; q < RU; ++q) {
-      if (r + q < u.nrt) {
+    for (int j = 0; j < NCT; ++j) {
+      if (j < u.nct) {
+        float d[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-        for (int j = 0; j < NCT; ++j) {
-          if (j < u.nct) {
-            float d[4] = {0.f, 0.f, 0.f, 0.f};
-            mma_a4(d, xf[q][0], vh[q][j].x, vh[q][j].y);  // X_hi V_hi
-            mma_a4(d, xf[q][1], vh[q][j].z, vh[q][j].w);
-            add4(acc[j], d);
-          }
+        for (int q = 0; q < RU; ++q) {
+          mma_a4(d, xf[q][0], vh[q][j].x, vh[q][j].y);  // X_hi V_hi (zero tiles past the unit's end)
+          mma_a4(d, xf[q][1], vh[q][j].z, vh[q][j].w);
         }
+        add4(acc[j], d);
       }
     }
   }
@@ -874,7 +893,7 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
   const int np = (int)members.size();
   std::vector<MxPanel> panels(np);
   std::vector<int> colL_u(pairs.size()), colH_u(pairs.size()), colL_v(pairs.size()), colH_v(pairs.size());
-  long long tiles = 0, t_tiles = 0, t_words = 0;
+  long long tiles = 0, t_tiles = 0, t_words = 0, t_blocks = 0;
   for (int p = 0; p < np; ++p) {
     long long sl = 0, sh_ = 0;
     for (const Side& m : members[p]) {
@@ -912,6 +931,8 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
     t_tiles += P.nct;
     P.tw0 = t_words;
     t_words += f32 ? (long long)P.nct * 128 : (long long)P.nctl * 128 + (long long)(P.nct - P.nctl) * 64;
+    P.tb0 = t_blocks;
+    t_blocks += P.nct + P.nctl;
   }
 
   // column sources and the projection's column map
@@ -999,6 +1020,47 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
                               : (int)(t_word(P.tw0, P.nctl, c) << 1) | ((c >> 3) >= P.nctl ? 1 : 0);
   for (size_t c = 0; c < mirror.size(); ++c) tslot[c] = mirror[c] >= 0 ? own[mirror[c]] : -1 - own[c];
   HM_TRY(upload(M.tslot, tslot, s));
+  if (!f32) {
+    // 128-column passes on tcgen05: the T blocks' column map, and phase 2's
+    // blocks of 4 row tiles with their sources
+    std::vector<int2> own_tc(mirror.size()), tslot_tc(mirror.size());
+    for (const MxPanel& P : panels)
+      for (int c = 0; c < P.nct * 8; ++c) {
+        const int j = c >> 3, cc = c & 7;
+        own_tc[P.t0 * 8 + c] = make_int2((int)((P.tb0 + j) * 8 + cc),
+                                         j < P.nctl ? (int)((P.tb0 + P.nct + j) * 8 + cc) : -1);
+      }
+    for (size_t c = 0; c < mirror.size(); ++c)
+      tslot_tc[c] = mirror[c] >= 0 ? own_tc[mirror[c]] : make_int2(-1 - own_tc[c].x, own_tc[c].y);
+    HM_TRY(upload(M.tslot_tc, tslot_tc, s));
+    std::vector<MxSeg> segs;
+    std::vector<int> seg_ptr(1, 0);
+    const int tend = M.p2_tile0 + M.p2_tiles;
+    for (int G0 = M.p2_tile0; G0 < tend; G0 += 4) {
+      const int nk = std::min(4, tend - G0);
+      for (int l = 1; l <= depth; ++l)
+        for (int k = 0; k < nk;) {
+          const int p = pan_of[((size_t)1 << l) - 1 + (tile_leaf[G0 + k] >> (depth - l))];
+          int k2 = k + 1;
+          while (k2 < nk && pan_of[((size_t)1 << l) - 1 + (tile_leaf[G0 + k2] >> (depth - l))] == p) ++k2;
+          if (p >= 0) segs.push_back(MxSeg{p, ((1 << k2) - 1) & ~((1 << k) - 1), G0 - panels[p].tile0});
+          k = k2;
+        }
+      for (int k = 0; k < nk;) {
+        const int x = tile_leaf[G0 + k];
+        int k2 = k + 1;
+        while (k2 < nk && tile_leaf[G0 + k2] == x) ++k2;
+        for (int q = dptr[x]; q < dptr[x + 1]; ++q)
+          segs.push_back(MxSeg{-1 - dblk[q], ((1 << k2) - 1) & ~((1 << k) - 1), G0 - dense[dblk[q]].row_tile0});
+        k = k2;
+      }
+      if ((int)segs.size() == seg_ptr.back()) segs.push_back(MxSeg{kSegZero, 0, 0});
+      seg_ptr.push_back((int)segs.size());
+    }
+    HM_TRY(upload(M.p2_segs, segs, s));
+    HM_TRY(upload(M.p2_seg_ptr, seg_ptr, s));
+    M.p2_blocks = (int)seg_ptr.size() - 1;
+  }
   HM_TRY(upload(M.dense, dense, s));
   HM_TRY(upload(M.leaf_dptr, dptr, s));
   HM_TRY(upload(M.leaf_dblk, dblk, s));
@@ -1211,8 +1273,32 @@ hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, int 
                                std::min(chunk_tiles, P.nrt - ch * chunk_tiles), ch});
   }
   // the largest units first, so that the small ones fill the tail
-  std::stable_sort(units.begin(), units.end(),
-                   [](const MxUnit& a, const MxUnit& b) { return a.nrt * a.nct > b.nrt * b.nct; });
+  auto larger = [](const MxUnit& a, const MxUnit& b) { return a.nrt * a.nct > b.nrt * b.nct; };
+  std::stable_sort(units.begin(), units.end(), larger);
+  // tcgen05 units (128-column passes): 16 column tiles, low-part tiles apart
+  std::vector<MxUnit> tcu;
+  if (M.fmt == 0) {
+    for (int p = 0; p < (int)panels.size(); ++p) {
+      const MxPanel& P = panels[p];
+      for (int part = 0; part < 2; ++part) {
+        const int c0 = part ? P.nctl : 0, c1 = part ? P.nct : P.nctl;
+        for (int c = c0; c < c1; c += 16)
+          for (int ch = 0; ch < P.nchunk; ++ch)
+            tcu.push_back(MxUnit{p, c, std::min(16, c1 - c), ch * chunk_tiles,
+                                 std::min(chunk_tiles, P.nrt - ch * chunk_tiles), ch});
+      }
+    }
+    std::stable_sort(tcu.begin(), tcu.end(), larger);
+    int dev = 0;
+    HM_CUDA(cudaGetDevice(&dev));
+    HM_CUDA(cudaDeviceGetAttribute(&M.num_sms, cudaDevAttrMultiProcessorCount, dev));
+    if (!M.tc_err.p) {
+      HM_TRY(M.tc_err.alloc(1));
+      HM_CUDA(cudaMemsetAsync(M.tc_err.p, 0, sizeof(int), s));
+    }
+  }
+  HM_TRY(upload(M.tc_units, tcu, s));
+  M.num_tc_units = (int)tcu.size();
   HM_TRY(upload(M.panels, panels, s));
   HM_TRY(upload(M.units, units, s));
   HM_TRY(upload(M.mtiles, mtiles, s));
@@ -1225,6 +1311,9 @@ hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, int 
   return HM_OK;
 }
 
+hm_status mixed_warp_pass(hm_hmatrix_s* h, int nh, int nr, uint4* Xf, float4* S, uint32_t* T, long long xh,
+                          long long sh, long long th, float* Y, int ldy, cudaStream_t s, KernelMarks* km);
+
 hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, float* Y, int ldy, float* scratch,
                           cudaStream_t s, KernelMarks* km) {
   MxPlan& M = h->mx;
@@ -1234,6 +1323,9 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
   const int nh = nr > 64 ? 8 : (nr > 32 ? 4 : (nr > 16 ? 2 : 1));
   // scratch: the parts' X fragments, then their chunk partials, then their T
   const long long xh = (long long)M.num_tiles * 128, sh = M.s_tiles * 32, th = M.t_words;
+  // (a 128-column pass on tcgen05: X's image where the fragments would be,
+  // T in blocks where the parts' T would be)
+  const bool tc = M.tc_pass(nh);
   uint4* Xf = reinterpret_cast<uint4*>(scratch);
   float4* S = reinterpret_cast<float4*>(Xf + nh * xh);
   uint32_t* T = reinterpret_cast<uint32_t*>(S + nh * sh);
@@ -1241,10 +1333,27 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
   const long long xbytes = 4ll * h->n * 16 * nh;  // the X fragments, hi + lo
   if (M.num_tiles > 0) {
     k_mx_split_x<<<dim3((M.num_tiles + 3) / 4, nh), 128, 0, s>>>(X, ldx, nr, M.num_tiles, M.tile_leaf.p,
-                                                                 M.leaf_tile0.p, leaf_off, Xf);
+                                                                 M.leaf_tile0.p, leaf_off, Xf, tc ? Xf : nullptr);
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_mx_split_x", 4ll * h->n * nr + xbytes, s);
   }
+  if (tc) {
+    HM_TRY(mixed_tc_pass(h, nr, Xf, S, sh, reinterpret_cast<uint4*>(T), Y, ldy, s, km));
+  } else {
+    HM_TRY(mixed_warp_pass(h, nh, nr, Xf, S, T, xh, sh, th, Y, ldy, s, km));
+  }
+  if (h->diag_fly)  // the diagonal from coordinates, 16 columns at a time
+    for (int c0 = 0; c0 < nr; c0 += 16)
+      HM_TRY(diag_fly_panel(h, std::min(16, nr - c0), X + (size_t)c0 * ldx, ldx, Y + (size_t)c0 * ldy, ldy, s, km));
+  return HM_OK;
+}
+
+// Phases 1 and 2 of a pass on the warp-level MMA kernels (nh parts of 16).
+hm_status mixed_warp_pass(hm_hmatrix_s* h, int nh, int nr, uint4* Xf, float4* S, uint32_t* T, long long xh,
+                          long long sh, long long th, float* Y, int ldy, cudaStream_t s, KernelMarks* km) {
+  MxPlan& M = h->mx;
+  const int* leaf_off = h->tree->offsets.p;
+  const long long xbytes = 4ll * h->n * 16 * nh;
   if (M.num_units > 0) {
     const unsigned nu = (unsigned)M.num_units;
     if (M.p1_ring && nh == 1 && M.group_tiles <= 4) {
@@ -1289,9 +1398,6 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
     HM_LAUNCH_CHECK();
     if (km) km->mark("k_mx_p2", M.bytes_p2 + xbytes + 4ll * h->n * nr, s);
   }
-  if (h->diag_fly)  // the diagonal from coordinates, 16 columns at a time
-    for (int c0 = 0; c0 < nr; c0 += 16)
-      HM_TRY(diag_fly_panel(h, std::min(16, nr - c0), X + (size_t)c0 * ldx, ldx, Y + (size_t)c0 * ldy, ldy, s, km));
   return HM_OK;
 }
 

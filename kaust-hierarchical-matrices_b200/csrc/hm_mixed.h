@@ -36,6 +36,7 @@ struct MxPanel {
   long long s0;                  // first phase-1 output tile (nchunk x nct tiles)
   long long t0;                  // first global factor column tile (nct tiles)
   long long tw0;                 // first 32-bit word of the panel's T (nctl tiles of 128 words, then 64 each)
+  long long tb0;                 // 128-column passes on tcgen05: first 2 KB block of its T (nct hi blocks, nctl lo)
   int nct, nctl;                 // 8-column tiles; the first nctl carry low parts
   int tile0, nrt;                // first global row tile, row tiles
   int nchunk;                    // row chunks of the projection
@@ -45,6 +46,18 @@ struct MxPanel {
 struct MxUnit {  // phase-1 work item, one warp: up to 8 column tiles x up to 64 row tiles
   int panel, ct0, nct, rt0, nrt, chunk;
 };
+
+// Phase 2 of a 128-column pass on tcgen05 works on blocks of 4 global row
+// tiles (128 rows); each block's sources, in the order they are added: the
+// ancestors' panels level by level (kind = panel), then the leaves' dense
+// blocks (kind = -1 - dense block); mask = the block's tiles (bit k) that
+// take part (the others' rows of A are zero); the source's row tile of the
+// block's tile k is rt_base + k.  kind = kSegZero: a block without sources
+// (its rows of Y are zero).
+struct MxSeg {
+  int kind, mask, rt_base;
+};
+constexpr int kSegZero = -0x7fffffff;
 
 struct MxDense {  // a dense block in P2 order, hi + lo, [row tile][col tile]
   long long hi, lo;
@@ -100,11 +113,29 @@ struct MxPlan {
   int chunk_tiles = 128, group_tiles = 4;  // phase-1 unit shape (schedule parameters)
   bool p1_ring = false;                    // phase 1 by persistent warps with a cp.async ring
   int num_sms = 148;
+  // 128-column passes (BF16 format) on tcgen05 (hm_mixed_tc.cu): phase-1
+  // units of up to 16 column tiles, split where a panel's low-part tiles end;
+  // T in 2 KB blocks (per 8 columns: 128 right-hand sides x 8 BF16, the
+  // K-major core-matrix layout); tslot_tc: per global factor column the
+  // destination's {hi, lo} position (block * 8 + column; lo -1 without a low
+  // part; a padding column: {-1 - own hi, own lo}); phase-2 blocks of 4 row
+  // tiles with their sources (p2_seg_ptr: CSR over p2_blocks blocks).
+  bool wide_tc = false;
+  DevBuf<MxUnit> tc_units;
+  int num_tc_units = 0;
+  DevBuf<int2> tslot_tc;
+  DevBuf<MxSeg> p2_segs;
+  DevBuf<int> p2_seg_ptr;
+  int p2_blocks = 0;
+  DevBuf<int> tc_err;  // set when a bounded wait of those kernels gave up
+  bool tc_pass(int halves) const { return wide_tc && fmt == 0 && halves == 8; }
   // scratch of one 16-column panel of right-hand sides, in floats: X
   // fragments, chunk partials, T (the projections by expanding column: BF16
   // hi + lo for the columns with low parts, hi for the others)
   // of a pass of `halves` such panels (1, 2, 4 or 8: up to 128 right-hand sides)
   // (FP32 format: X as TF32 hi + lo, 8 words per lane and tile instead of 4)
+  // (a tcgen05 pass keeps X's image, 16 KB per row tile, where the eight
+  // parts' fragments would be, and T in blocks where the parts' T would be)
   long long scratch_floats(int halves = 1) const {
     return (((long long)num_tiles * (fmt ? 8 : 4) + s_tiles) * 128 + t_words) * halves;
   }
@@ -125,6 +156,13 @@ struct MxDenseIn {
 // the phase-1 units and the column map of the projection.
 hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const std::vector<MxDenseIn>& dense,
                       cudaStream_t s);
+
+// A 128-column pass on tcgen05 after k_mx_split_x wrote Xtc (16 KB per row
+// tile): phase 1 (T as blocks, or chunk partials S, sh in float4 per part),
+// the chunk reduction, phase 2 (Y, tree order, nr <= 128 columns).
+struct KernelMarks;
+hm_status mixed_tc_pass(hm_hmatrix_s* h, int nr, const uint4* Xtc, float4* S, long long sh, uint4* Tb, float* Y,
+                        int ldy, cudaStream_t s, KernelMarks* km);
 
 struct KernelMarks;
 

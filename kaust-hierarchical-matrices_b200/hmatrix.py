@@ -104,6 +104,7 @@ def lib():
             L.hm_hmatvec_f64.argtypes = [P, I, I, P, I, P, I, I, P]
             L.hm_kdtree_build_div.argtypes = [P, I, I, I, I, P, ctypes.POINTER(P)]
             L.hm_hmatrix_stats_get.argtypes = [P, ctypes.POINTER(Stats)]
+            L.hm_hmatrix_check.argtypes = [P, P]
             L.hm_hmatvec.argtypes = [P, I, I, P, I, P, I, I, P]
             L.hm_hmatrix_free.argtypes = [P]
             L.hm_hmatrix_blocks.argtypes = [P, P, P, P, P]
@@ -285,6 +286,11 @@ class HMatrix:
         out = {k: getattr(st, k) for k, _ in Stats._fields_ if k != "phase_seconds"}
         out["phase_seconds"] = dict(zip(Stats.PHASES, list(st.phase_seconds)))
         return out
+
+    def check(self, stream=None):
+        """Wait for the stream and raise if a bounded device-side wait of a
+        product kernel gave up since the last check (hm_hmatrix_check)."""
+        _check(lib().hm_hmatrix_check(self.h, _stream(stream)))
 
     def matvec(self, X, Y=None, trans=0, original_order=False, stream=None):
         """Y = H X for a float32 CUDA tensor X of shape (n, nrhs), column-major
