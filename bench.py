@@ -329,7 +329,8 @@ def kernel_times(hm, lib, H, X, Y, n, nrhs, stream, reps=6):
     return [(k, acc[k][0], acc[k][1]) for k in order]
 
 
-TRAFFIC_SOURCES = ["csrc/hm_mixed.cu", "csrc/hm_mixed.h", "csrc/hm_fp32.cu", "csrc/hm_mma.cuh", "csrc/hm_matvec.cu"]
+TRAFFIC_SOURCES = ["csrc/hm_mixed.cu", "csrc/hm_mixed.h", "csrc/hm_fp32.cu", "csrc/hm_mma.cuh", "csrc/hm_matvec.cu",
+                   "csrc/hm_mixed_tc.cu", "csrc/hm_tc.cuh"]
 
 
 def kernel_source_digest():

@@ -409,12 +409,13 @@ HM_API hm_status hm_autotune(hm_hmatrix h, int nrhs, const char* cache_path, voi
                              char* choice, int choice_len);
 
 /* Applies a schedule given as hm_autotune describes it, e.g.
- * "mixed chunk_tiles=64 group_tiles=8 p1_ring=1 wide_tc=1", "fp32 chunk_tiles=32
- * group_tiles=4" (FP32 panels) or "fp32 p1_rows=256" (FP32 per-block
- * kernels; they read the FP32 factors, which FP32 matrices keep).  For the
- * mixed form, wide_tc (optional; 0 by default) selects tcgen05 kernels for
- * both phases of passes of 65-128 right-hand sides (0: the warp-level MMA
- * kernels, the faster of the two as measured). */
+ * "mixed chunk_tiles=64 group_tiles=8 p1_ring=1 wide_tc=1 tc_chunk=32",
+ * "fp32 chunk_tiles=32 group_tiles=4" (FP32 panels) or "fp32 p1_rows=256"
+ * (FP32 per-block kernels; they read the FP32 factors, which FP32 matrices
+ * keep).  For the mixed form, wide_tc and tc_chunk are optional: wide_tc = 1
+ * (the default) runs passes of 65-128 right-hand sides on tcgen05 kernels
+ * (tensor memory accumulators), whose phase-1 units span tc_chunk row tiles
+ * (default 32); wide_tc = 0 runs them on the warp-level MMA kernels. */
 HM_API hm_status hm_schedule_set(hm_hmatrix h, const char* choice, void* stream);
 
 /* --- Batches of independent clouds ------------------------------------------

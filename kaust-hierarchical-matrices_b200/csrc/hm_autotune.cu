@@ -37,8 +37,8 @@ bool is_mixed(hm_hmatrix h) { return h->opts.precision == HM_PREC_MIXED; }
 std::string describe(hm_hmatrix h, const Choice& c) {
   char buf[96];
   if (is_mixed(h))
-    std::snprintf(buf, sizeof buf, "mixed chunk_tiles=%d group_tiles=%d p1_ring=%d wide_tc=%d", c.a, c.b, c.c,
-                  c.d >= 0 ? c.d : (h->mx.wide_tc ? 1 : 0));
+    std::snprintf(buf, sizeof buf, "mixed chunk_tiles=%d group_tiles=%d p1_ring=%d wide_tc=%d tc_chunk=%d", c.a, c.b,
+                  c.c, c.d >= 0 ? c.d : (h->mx.wide_tc ? 1 : 0), h->mx.tc_chunk_tiles);
   else if (c.b > 0)
     std::snprintf(buf, sizeof buf, "fp32 chunk_tiles=%d group_tiles=%d", c.a, c.b);
   else
@@ -165,9 +165,14 @@ extern "C" hm_status hm_schedule_set(hm_hmatrix h, const char* choice, void* str
   if (!h || !choice) return fail(HM_ERR_INVALID, "hm_schedule_set: null argument");
   Choice c;
   if (is_mixed(h)) {
-    const int got = std::sscanf(choice, "mixed chunk_tiles=%d group_tiles=%d p1_ring=%d wide_tc=%d", &c.a, &c.b,
-                                &c.c, &c.d);
-    if (got < 3 || (got == 4 && c.d != 0 && c.d != 1))
+    int tcc = 0;
+    const int got = std::sscanf(choice, "mixed chunk_tiles=%d group_tiles=%d p1_ring=%d wide_tc=%d tc_chunk=%d", &c.a,
+                                &c.b, &c.c, &c.d, &tcc);
+    if (got == 5) {
+      if (tcc < 1) return fail(HM_ERR_INVALID, std::string("hm_schedule_set: tc_chunk must be >= 1: ") + choice);
+      h->mx.tc_chunk_tiles = tcc;
+    }
+    if (got < 3 || (got >= 4 && c.d != 0 && c.d != 1))
       return fail(HM_ERR_INVALID, std::string("hm_schedule_set: not a mixed-form schedule: ") + choice);
   } else if (std::sscanf(choice, "fp32 chunk_tiles=%d group_tiles=%d", &c.a, &c.b) == 2) {
     if (c.b < 1 || c.b > 8)

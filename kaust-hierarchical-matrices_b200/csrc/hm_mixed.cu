@@ -37,6 +37,17 @@ namespace hm {
 namespace {
 
 
+// A P1 tile (32 rows x 8 columns of a factor) keeps lane (g,t)'s 16 bytes
+// -- column g at rows rho(t, 0..7) -- at word 4 g + (t ^ ((g >> 1) & 3)): the
+// K-major core-matrix layout with the 64-byte swizzle (column g's 64-byte row
+// at 64 g, its K block t at 16-byte chunk t ^ ((g >> 1) & 3)), so that a run
+// of tiles is a tcgen05 operand image as stored.  The 4 lanes of a column
+// only trade places: each quarter-warp still reads one 128-byte line.
+__host__ __device__ __forceinline__ int p1_slot(int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  return 4 * g + (t ^ ((g >> 1) & 3));
+}
+
 __device__ __forceinline__ void mma_a4(float (&d)[4], const uint4& a, uint32_t b0, uint32_t b1) {
   mma_bf16(d, a.x, a.y, a.z, a.w, b0, b1);
 }
@@ -210,8 +221,8 @@ __device__ __forceinline__ void mx_p1_unit(const MxUnit& u, const MxPanel& P, co
 #pragma unroll
         for (int p = 0; p < 4; ++p)  // X's low part only for units with low-part columns
           xf[q][h][p] = ok && (p < 2 || xlo) ? ld_keep(xp + h * xh + p * 32, keep) : z;
-      const uint4* hp = store + (P.hi1 + rt * P.nct + u.ct0) * 32 + lane;
-      const uint4* lp = store + (P.lo1 + rt * P.nctl + u.ct0) * 32 + lane;
+      const uint4* hp = store + (P.hi1 + rt * P.nct + u.ct0) * 32 + p1_slot(lane);
+      const uint4* lp = store + (P.lo1 + rt * P.nctl + u.ct0) * 32 + p1_slot(lane);
 #pragma unroll
       for (int j = 0; j < NCT; ++j) {
         vh[q][j] = ok && j < u.nct ? ld_tile<SH>(hp + j * 32) : z;
@@ -286,7 +297,7 @@ __device__ __forceinline__ void mx_p1_unit_hi(const MxUnit& u, const MxPanel& P,
       const uint4* xp = Xf + (size_t)(P.tile0 + rt) * 128 + lane;
       xf[q][0] = ok ? ld_keep(xp, keep) : z;
       xf[q][1] = ok ? ld_keep(xp + 32, keep) : z;
-      const uint4* hp = store + (P.hi1 + rt * P.nct + u.ct0) * 32 + lane;
+      const uint4* hp = store + (P.hi1 + rt * P.nct + u.ct0) * 32 + p1_slot(lane);
 #pragma unroll
       for (int j = 0; j < NCT; ++j) vh[q][j] = ok && j < u.nct ? __ldcs(hp + j * 32) : z;
     }
@@ -428,10 +439,10 @@ __global__ void __launch_bounds__(32 * WARPS, 1) k_mx_p1r(const MxUnit* __restri
       const uint4* xp = Xf + (size_t)(PP.tile0 + rt) * 128 + lane;
 #pragma unroll
       for (int p = 0; p < 4; ++p) cp16(base + (uint32_t)(p * 32) * 16u, xp + p * 32);
-      const uint4* hp = store + (PP.hi1 + rt * PP.nct + U.ct0) * 32 + lane;
+      const uint4* hp = store + (PP.hi1 + rt * PP.nct + U.ct0) * 32 + p1_slot(lane);
       for (int j = 0; j < U.nct; ++j) cp16(base + (uint32_t)((4 + j) * 32) * 16u, hp + j * 32);
       const int nl = min(U.nct, max(0, PP.nctl - U.ct0));
-      const uint4* lp = store + (PP.lo1 + rt * PP.nctl + U.ct0) * 32 + lane;
+      const uint4* lp = store + (PP.lo1 + rt * PP.nctl + U.ct0) * 32 + p1_slot(lane);
       for (int j = 0; j < nl; ++j) cp16(base + (uint32_t)((4 + VT + j) * 32) * 16u, lp + j * 32);
       if (++prt == U.nrt) {
         prt = 0;
@@ -771,10 +782,10 @@ __global__ void k_mx_conv_panels(const MxPanel* __restrict__ panels, const long 
   split_bf16x2(val(g + 8, cp2), val(g + 8, cp2 + 1), h2.y, l2.y);
   split_bf16x2(val(g + 16, cp2), val(g + 16, cp2 + 1), h2.z, l2.z);
   split_bf16x2(val(g + 24, cp2), val(g + 24, cp2 + 1), h2.w, l2.w);
-  store[(P.hi1 + (long long)rt * P.nct + ct) * 32 + lane] = h1;
+  store[(P.hi1 + (long long)rt * P.nct + ct) * 32 + p1_slot(lane)] = h1;
   store[(P.hi2 + (long long)rt * P.nct + ct) * 32 + lane] = h2;
   if (ct < P.nctl) {
-    store[(P.lo1 + (long long)rt * P.nctl + ct) * 32 + lane] = l1;
+    store[(P.lo1 + (long long)rt * P.nctl + ct) * 32 + p1_slot(lane)] = l1;
     store[(P.lo2 + (long long)rt * P.nctl + ct) * 32 + lane] = l2;
   }
 }
@@ -1033,9 +1044,21 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
     for (size_t c = 0; c < mirror.size(); ++c)
       tslot_tc[c] = mirror[c] >= 0 ? own_tc[mirror[c]] : make_int2(-1 - own_tc[c].x, own_tc[c].y);
     HM_TRY(upload(M.tslot_tc, tslot_tc, s));
-    std::vector<MxSeg> segs;
-    std::vector<int> seg_ptr(1, 0);
+    std::vector<P2Step> steps;
+    std::vector<int> step_ptr(1, 0);
     const int tend = M.p2_tile0 + M.p2_tiles;
+    auto mask_of = [](int k, int k2) { return ((1 << k2) - 1) & ~((1 << k) - 1); };
+    auto add_panel = [&](int p, int mask, int G0) {
+      const MxPanel& P = panels[p];
+      const long long rb = G0 - P.tile0;  // the panel's row tile of the block's tile 0
+      for (int j0 = 0; j0 < P.nctl; j0 += 4)
+        steps.push_back(P2Step{P.hi2 + rb * P.nct + j0, P.lo2 + rb * P.nctl + j0, (P.tb0 + j0) * 128,
+                               (P.tb0 + P.nct + j0) * 128, P.nct, P.nctl,
+                               0 | (std::min(4, P.nctl - j0) << 2) | (mask << 8), 0});
+      for (int j0 = P.nctl; j0 < P.nct; j0 += 8)
+        steps.push_back(P2Step{P.hi2 + rb * P.nct + j0, -1, (P.tb0 + j0) * 128, -1, P.nct, 0,
+                               1 | (std::min(8, P.nct - j0) << 2) | (mask << 8), 0});
+    };
     for (int G0 = M.p2_tile0; G0 < tend; G0 += 4) {
       const int nk = std::min(4, tend - G0);
       for (int l = 1; l <= depth; ++l)
@@ -1043,23 +1066,29 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
           const int p = pan_of[((size_t)1 << l) - 1 + (tile_leaf[G0 + k] >> (depth - l))];
           int k2 = k + 1;
           while (k2 < nk && pan_of[((size_t)1 << l) - 1 + (tile_leaf[G0 + k2] >> (depth - l))] == p) ++k2;
-          if (p >= 0) segs.push_back(MxSeg{p, ((1 << k2) - 1) & ~((1 << k) - 1), G0 - panels[p].tile0});
+          if (p >= 0) add_panel(p, mask_of(k, k2), G0);
           k = k2;
         }
       for (int k = 0; k < nk;) {
         const int x = tile_leaf[G0 + k];
         int k2 = k + 1;
         while (k2 < nk && tile_leaf[G0 + k2] == x) ++k2;
-        for (int q = dptr[x]; q < dptr[x + 1]; ++q)
-          segs.push_back(MxSeg{-1 - dblk[q], ((1 << k2) - 1) & ~((1 << k) - 1), G0 - dense[dblk[q]].row_tile0});
+        for (int q = dptr[x]; q < dptr[x + 1]; ++q) {
+          const MxDense& D = dense[dblk[q]];
+          const long long rb = G0 - D.row_tile0;
+          for (int j0 = 0; j0 < D.nct; j0 += 4)
+            steps.push_back(P2Step{D.hi + rb * D.nct + j0, D.lo + rb * D.nct + j0,
+                                   (long long)(D.col_tile0 + j0 / 4) * 1024, (long long)(D.col_tile0 + j0 / 4) * 1024 + 512,
+                                   D.nct, D.nct, 2 | (4 << 2) | (mask_of(k, k2) << 8), 0});
+        }
         k = k2;
       }
-      if ((int)segs.size() == seg_ptr.back()) segs.push_back(MxSeg{kSegZero, 0, 0});
-      seg_ptr.push_back((int)segs.size());
+      if ((int)steps.size() == step_ptr.back()) steps.push_back(P2Step{0, -1, 0, -1, 0, 0, 3, 0});
+      step_ptr.push_back((int)steps.size());
     }
-    HM_TRY(upload(M.p2_segs, segs, s));
-    HM_TRY(upload(M.p2_seg_ptr, seg_ptr, s));
-    M.p2_blocks = (int)seg_ptr.size() - 1;
+    HM_TRY(upload(M.p2_steps, steps, s));
+    HM_TRY(upload(M.p2_step_ptr, step_ptr, s));
+    M.p2_blocks = (int)step_ptr.size() - 1;
   }
   HM_TRY(upload(M.dense, dense, s));
   HM_TRY(upload(M.leaf_dptr, dptr, s));
@@ -1275,20 +1304,47 @@ hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, int 
   // the largest units first, so that the small ones fill the tail
   auto larger = [](const MxUnit& a, const MxUnit& b) { return a.nrt * a.nct > b.nrt * b.nct; };
   std::stable_sort(units.begin(), units.end(), larger);
-  // tcgen05 units (128-column passes): 16 column tiles, low-part tiles apart
-  std::vector<MxUnit> tcu;
+  // tcgen05 units (128-column passes): 16 column tiles, low-part tiles apart,
+  // over row chunks of their own size, with their own partials
+  std::vector<TcUnit> tcu;
+  std::vector<int2> mtiles_tc;
+  long long s_tiles_tc = 0;
   if (M.fmt == 0) {
+    const int tch = std::max(1, M.tc_chunk_tiles);
     for (int p = 0; p < (int)panels.size(); ++p) {
-      const MxPanel& P = panels[p];
+      MxPanel& P = panels[p];
+      P.nchunkt = std::max(1, (P.nrt + tch - 1) / tch);
+      P.s0t = s_tiles_tc;
+      if (P.nchunkt > 1) {
+        s_tiles_tc += (long long)P.nchunkt * P.nct;
+        for (int c = 0; c < P.nct; ++c) mtiles_tc.push_back(make_int2(p, c));
+      }
       for (int part = 0; part < 2; ++part) {
         const int c0 = part ? P.nctl : 0, c1 = part ? P.nct : P.nctl;
         for (int c = c0; c < c1; c += 16)
-          for (int ch = 0; ch < P.nchunk; ++ch)
-            tcu.push_back(MxUnit{p, c, std::min(16, c1 - c), ch * chunk_tiles,
-                                 std::min(chunk_tiles, P.nrt - ch * chunk_tiles), ch});
+          for (int ch = 0; ch < P.nchunkt; ++ch) {
+            TcUnit t{};
+            const int rt0 = ch * tch;
+            t.nct = std::min(16, c1 - c);
+            t.nrt = std::min(tch, P.nrt - rt0);
+            t.shi = P.nct;
+            t.slo = P.nctl;
+            t.vhi = P.hi1 + (long long)rt0 * P.nct + c;
+            t.vlo = part ? -1 : P.lo1 + (long long)rt0 * P.nctl + c;
+            t.xtile = P.tile0 + rt0;
+            t.flags = (part ? 0 : 1) | (P.nchunkt == 1 ? 2 : 0);
+            t.out = P.nchunkt == 1 ? P.t0 + c : P.s0t + (long long)ch * P.nct + c;
+            tcu.push_back(t);
+          }
       }
     }
-    std::stable_sort(tcu.begin(), tcu.end(), larger);
+    // in row order (the larger unit first among those that start on the same
+    // row tile): the CTAs, each walking every gridDim-th unit, then work on
+    // nearby rows at every level at once, and X's image of those rows is
+    // read from HBM about once for all levels (it stays in L2 between them)
+    std::stable_sort(tcu.begin(), tcu.end(), [](const TcUnit& a, const TcUnit& b) {
+      return a.xtile != b.xtile ? a.xtile < b.xtile : a.nrt > b.nrt;
+    });
     int dev = 0;
     HM_CUDA(cudaGetDevice(&dev));
     HM_CUDA(cudaDeviceGetAttribute(&M.num_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -1298,7 +1354,10 @@ hm_status mixed_schedule(hm_hmatrix_s* h, int chunk_tiles, int group_tiles, int 
     }
   }
   HM_TRY(upload(M.tc_units, tcu, s));
+  HM_TRY(upload(M.mtiles_tc, mtiles_tc, s));
   M.num_tc_units = (int)tcu.size();
+  M.nmt_tc = (long long)mtiles_tc.size();
+  M.s_tiles_tc = s_tiles_tc;
   HM_TRY(upload(M.panels, panels, s));
   HM_TRY(upload(M.units, units, s));
   HM_TRY(upload(M.mtiles, mtiles, s));
@@ -1328,7 +1387,9 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
   const bool tc = M.tc_pass(nh);
   uint4* Xf = reinterpret_cast<uint4*>(scratch);
   float4* S = reinterpret_cast<float4*>(Xf + nh * xh);
-  uint32_t* T = reinterpret_cast<uint32_t*>(S + nh * sh);
+  // (the tcgen05 pass's partials, 4 KB per tile of its own chunking, may take more room)
+  const long long s_room = tc ? std::max(M.s_tiles, M.s_tiles_tc) * 32 : sh;
+  uint32_t* T = reinterpret_cast<uint32_t*>(S + nh * s_room);
   const int* leaf_off = h->tree->offsets.p;
   const long long xbytes = 4ll * h->n * 16 * nh;  // the X fragments, hi + lo
   if (M.num_tiles > 0) {
@@ -1338,7 +1399,7 @@ hm_status mixed_run_panel(hm_hmatrix_s* h, int nr, const float* X, int ldx, floa
     if (km) km->mark("k_mx_split_x", 4ll * h->n * nr + xbytes, s);
   }
   if (tc) {
-    HM_TRY(mixed_tc_pass(h, nr, Xf, S, sh, reinterpret_cast<uint4*>(T), Y, ldy, s, km));
+    HM_TRY(mixed_tc_pass(h, nr, Xf, reinterpret_cast<float*>(S), reinterpret_cast<uint4*>(T), Y, ldy, s, km));
   } else {
     HM_TRY(mixed_warp_pass(h, nh, nr, Xf, S, T, xh, sh, th, Y, ldy, s, km));
   }

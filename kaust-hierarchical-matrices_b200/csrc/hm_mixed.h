@@ -16,6 +16,8 @@
 // warp load.  Two such orders exist per factor:
 //   P1 (phase 1, the factor is the B operand of X^T V, pairs along rows):
 //     lane (g,t) = {V[2t,2t+1][g], V[2t+8,2t+9][g], V[16+2t,17+2t][g], V[24+2t,25+2t][g]}
+//     at word 4 g + (t ^ ((g >> 1) & 3)) (the 64-byte-swizzled core-matrix
+//     order, so that runs of tiles are tcgen05 operand images)
 //   P2 (phase 2, the factor is the A operand of U T, pairs along columns):
 //     lane (g,t) = {U[g][2t,2t+1], U[g+8][2t,2t+1], U[g+16][2t,2t+1], U[g+24][2t,2t+1]}
 // (g = lane / 4, t = lane % 4; each pair is bf16x2 with the lower index in the
@@ -23,6 +25,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "hm_internal.h"
@@ -40,6 +43,8 @@ struct MxPanel {
   int nct, nctl;                 // 8-column tiles; the first nctl carry low parts
   int tile0, nrt;                // first global row tile, row tiles
   int nchunk;                    // row chunks of the projection
+  int nchunkt;                   // the same in a 128-column pass on tcgen05 (its own chunk size)
+  long long s0t;                 // its first chunk-partial tile there
   int r0;                        // first (tree-order) row of the cluster
 };
 
@@ -47,17 +52,35 @@ struct MxUnit {  // phase-1 work item, one warp: up to 8 column tiles x up to 64
   int panel, ct0, nct, rt0, nrt, chunk;
 };
 
-// Phase 2 of a 128-column pass on tcgen05 works on blocks of 4 global row
-// tiles (128 rows); each block's sources, in the order they are added: the
-// ancestors' panels level by level (kind = panel), then the leaves' dense
-// blocks (kind = -1 - dense block); mask = the block's tiles (bit k) that
-// take part (the others' rows of A are zero); the source's row tile of the
-// block's tile k is rt_base + k.  kind = kSegZero: a block without sources
-// (its rows of Y are zero).
-struct MxSeg {
-  int kind, mask, rt_base;
+// A phase-1 unit of the tcgen05 kernel with the panel fields it needs (one
+// load per unit): up to 16 column tiles of one kind (with or without low parts).
+struct TcUnit {
+  long long vhi;  // P1 hi tile (512-byte units) of its first column tile at its first row tile
+  long long vlo;  // the same for the low parts (units with low parts)
+  long long out;  // T (panel in one row chunk): its first global column tile; else its first S tile
+  int shi, slo;   // tiles per row tile of the panel: nct, nctl
+  int nct, nrt;   // column tiles (<= 16), row tiles
+  int xtile;      // global row tile of its first row (X's image)
+  int flags;      // 1: columns with low parts; 2: T (else chunk partials S)
 };
-constexpr int kSegZero = -0x7fffffff;
+
+// Phase 2 of a 128-column pass on tcgen05 works on blocks of 4 global row
+// tiles (128 rows).  Each block's sources, in the order they are added --
+// the ancestors' panels level by level, then the leaves' dense blocks -- are
+// cut into steps (host-built):
+//   kind 0: up to 4 column tiles of a panel with low parts (A hi + lo, T hi + lo)
+//   kind 1: up to 8 column tiles of a panel without (A hi, T hi)
+//   kind 2: 4 column tiles (32 columns) of a dense block (A hi + lo, X's image)
+//   kind 3: nothing (a block without sources: its rows of Y are zero)
+// A rows of the block's tiles that the source does not cover (mask bit k
+// clear) are zero.
+struct P2Step {
+  long long a_hi, a_lo;  // P2 tile (512-byte units) of the block's tile 0 at the step's first column tile
+  long long b_hi, b_lo;  // 16-byte offset of B: T blocks (kinds 0, 1) or X's image (kind 2)
+  int a_stride, a_stride_lo;  // tiles per row tile of the source (hi, lo)
+  int info;                   // kind | column tiles << 2 | mask << 8
+  int pad;
+};
 
 struct MxDense {  // a dense block in P2 order, hi + lo, [row tile][col tile]
   long long hi, lo;
@@ -119,13 +142,16 @@ struct MxPlan {
   // K-major core-matrix layout); tslot_tc: per global factor column the
   // destination's {hi, lo} position (block * 8 + column; lo -1 without a low
   // part; a padding column: {-1 - own hi, own lo}); phase-2 blocks of 4 row
-  // tiles with their sources (p2_seg_ptr: CSR over p2_blocks blocks).
-  bool wide_tc = false;
-  DevBuf<MxUnit> tc_units;
+  // tiles with their steps (p2_step_ptr: CSR over p2_blocks blocks).
+  bool wide_tc = true;
+  int tc_chunk_tiles = 32;         // row tiles per tcgen05 phase-1 unit
+  DevBuf<int2> mtiles_tc;          // (panel, column tile) of panels of several tcgen05 row chunks
+  long long nmt_tc = 0, s_tiles_tc = 0;
+  DevBuf<TcUnit> tc_units;
   int num_tc_units = 0;
   DevBuf<int2> tslot_tc;
-  DevBuf<MxSeg> p2_segs;
-  DevBuf<int> p2_seg_ptr;
+  DevBuf<P2Step> p2_steps;
+  DevBuf<int> p2_step_ptr;
   int p2_blocks = 0;
   DevBuf<int> tc_err;  // set when a bounded wait of those kernels gave up
   bool tc_pass(int halves) const { return wide_tc && fmt == 0 && halves == 8; }
@@ -135,9 +161,11 @@ struct MxPlan {
   // of a pass of `halves` such panels (1, 2, 4 or 8: up to 128 right-hand sides)
   // (FP32 format: X as TF32 hi + lo, 8 words per lane and tile instead of 4)
   // (a tcgen05 pass keeps X's image, 16 KB per row tile, where the eight
-  // parts' fragments would be, and T in blocks where the parts' T would be)
+  // parts' fragments would be, its chunk partials, 4 KB per tile, where the
+  // parts' partials would be, and T in blocks where the parts' T would be)
   long long scratch_floats(int halves = 1) const {
-    return (((long long)num_tiles * (fmt ? 8 : 4) + s_tiles) * 128 + t_words) * halves;
+    const long long st = tc_pass(halves) ? std::max(s_tiles, s_tiles_tc) : s_tiles;
+    return (((long long)num_tiles * (fmt ? 8 : 4) + st) * 128 + t_words) * halves;
   }
 };
 
@@ -158,11 +186,11 @@ hm_status mixed_build(hm_hmatrix_s* h, const std::vector<MxPair>& pairs, const s
                       cudaStream_t s);
 
 // A 128-column pass on tcgen05 after k_mx_split_x wrote Xtc (16 KB per row
-// tile): phase 1 (T as blocks, or chunk partials S, sh in float4 per part),
+// tile): phase 1 (T as blocks, or chunk partials S: 128 floats per column),
 // the chunk reduction, phase 2 (Y, tree order, nr <= 128 columns).
 struct KernelMarks;
-hm_status mixed_tc_pass(hm_hmatrix_s* h, int nr, const uint4* Xtc, float4* S, long long sh, uint4* Tb, float* Y,
-                        int ldy, cudaStream_t s, KernelMarks* km);
+hm_status mixed_tc_pass(hm_hmatrix_s* h, int nr, const uint4* Xtc, float* S, uint4* Tb, float* Y, int ldy,
+                        cudaStream_t s, KernelMarks* km);
 
 struct KernelMarks;
 

@@ -54,6 +54,33 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_
   return true;
 }
 
+// As mbar_wait, but also gives up as soon as *abort (shared memory) is set.
+__device__ __forceinline__ bool mbar_wait_or(uint32_t bar, uint32_t parity, const volatile int* abort,
+                                             uint64_t limit_ns = 2000000000ull) {
+  if (mbar_test(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_test(bar, parity)) {
+    if (*abort || global_ns() - t0 > limit_ns) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+// Arrives once and adds `bytes` to the transaction count the phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// ---- bulk copies (TMA engine, no tensor map): global -> this CTA's shared
+// memory, both addresses 16-byte aligned, size a multiple of 16; completion
+// adds the bytes to the mbarrier's transaction count.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
 // ---- cp.async (16 bytes per thread, any shared-memory destination) -------------
 __device__ __forceinline__ void cpa16(uint32_t saddr, const void* g) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(g) : "memory");
@@ -94,6 +121,14 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 __device__ __forceinline__ uint64_t tc_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// The same for the K-major layout with the 64-byte swizzle (layout type 4 in
+// bits 61-63): rows of 64 bytes, 16-byte chunk c of row r at chunk
+// c ^ ((r >> 1) & 3); SBO = the stride of 8-row groups; LBO unused (1).
+__device__ __forceinline__ uint64_t tc_sdesc_sw64(uint32_t saddr, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) |
+         (4ull << 61);
 }
 
 // Instruction descriptor of kind::f16: D FP32 (bits 4-5 = 1), A and B BF16

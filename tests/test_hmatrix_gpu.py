@@ -292,10 +292,10 @@ def test_mixed_two_half_passes_match_single_passes(hm, diag_from_coords):
     """The mixed form multiplies up to 128 right-hand sides per pass: parts of
     16 share every factor tile read (two or four parts per warp; beyond 64
     right-hand sides, and in phase 2 beyond 32, the warps of a CTA share the
-    tiles).  Products of 40 (four parts) and 100 columns (eight parts) equal
-    the same columns multiplied 16 at a time, in tree order and in the points'
-    original order, with the diagonal blocks stored or generated from
-    coordinates."""
+    tiles).  Products of 40 (four parts) and 100 columns (eight parts, on the
+    tcgen05 kernels) equal the same columns multiplied 16 at a time, in tree
+    order and in the points' original order, with the diagonal blocks stored
+    or generated from coordinates."""
     import torch
 
     n, d, b = 24000, 3, 64
@@ -313,7 +313,11 @@ def test_mixed_two_half_passes_match_single_passes(hm, diag_from_coords):
                      for c0 in range(0, ncol, 16)]
             Ys = torch.cat(parts, dim=1)
             scale = torch.linalg.norm(Ys).item()
-            assert torch.linalg.norm(Y - Ys).item() <= 1e-6 * scale, (ncol, orig)
+            # 40 columns: the warp-level kernels, the same sums as 16 at a time
+            # up to their order; 100 columns: the tcgen05 kernels, whose MMA
+            # chains in tensor memory (not rounded to nearest) differ by ~1e-6
+            bound = 1e-6 if ncol <= 64 else 3e-6
+            assert torch.linalg.norm(Y - Ys).item() <= bound * scale, (ncol, orig)
 
 
 def test_reference_level_schedule(hm):
