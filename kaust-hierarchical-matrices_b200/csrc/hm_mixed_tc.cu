@@ -382,11 +382,12 @@ __device__ __forceinline__ void cpa4_zero(uint32_t saddr, const void* g) {
 }
 
 // A's image of the block's 4 row tiles x nk K blocks (column tiles j0 + jj),
-// word W of the tiles per producer thread (tile W / 128, jj-major; word
-// W % 128): word w of lane (g, t) of tile (k, jj) = rows g + 8 w of row tile
-// k at columns 2t, 2t+1 -> 16 g + 128 (4 k + w) + (DENSE ? 4 jj + 2048 t :
-// 4 t + 2048 jj).  Rows of tiles outside the mask, and K blocks cnt .. nk - 1,
-// are zero.
+// word W of the tiles per copy thread (tile W / 128, jj-major; word W % 128):
+// word w of lane (g, t) of tile (k, jj) = rows g + 8 w of row tile k at
+// columns 2t, 2t+1 -> 16 g + 128 (4 k + w) + (DENSE ? 4 jj + 2048 t : 4 t +
+// 2048 jj).  Rows of tiles outside the mask, and K blocks cnt .. nk - 1, are
+// zero.  (Measured: more copy warps raise the rate; fewer instructions per
+// copy with fewer warps, or 16-byte zeroing of whole masked row tiles, did not.)
 template <bool DENSE>
 __device__ __forceinline__ void p2_copy_a(uint32_t base, const uint4* __restrict__ store, long long a0, int stride,
                                           int mask, int cnt, int nk, int pt) {
