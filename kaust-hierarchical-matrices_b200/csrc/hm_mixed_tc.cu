@@ -350,8 +350,8 @@ __global__ void k_mx_reduce_tc(const int2* __restrict__ mtiles, long long nmt, c
 }
 
 // ---- phase 2 ------------------------------------------------------------------
-// Warp roles as in phase 1, with seven copy warps and eight drain warps (64
-// columns each): A (the factor tiles in
+// Warp roles as in phase 1, with 27 copy warps and four drain warps that keep
+// the running sums in tensor memory: A (the factor tiles in
 // P2 order) is rearranged word by word into its core-matrix image by
 // cp.async (4 bytes, any destination); B (T blocks, X's image) comes by bulk
 // copies from producer thread 0.  A producer thread's copies of step j are
@@ -366,11 +366,12 @@ __global__ void k_mx_reduce_tc(const int2* __restrict__ mtiles, long long nmt, c
 // 2 (n % 8) + 128 (n / 8), column c at 16 c; SBO 128, LBO 2048), X's image
 // K-major (n at 16 (n % 8) + 128 (n / 8); SBO 128, LBO 2048).
 constexpr int kP2Stages = 6;
-constexpr int kP2Bufs = 4;
+constexpr int kP2Bufs = 2;        // TMEM chain accumulators (columns 0-255); running sums at 256-383
 constexpr int kP2Chain = 4;      // steps per MMA chain
 constexpr int kP2Delay = 3;      // steps between a producer's copies and its arrival
-constexpr int kP2Producers = 224;  // threads of the copy warps 0-6
-constexpr int kP2Threads = 512;    // copy warps 0-6, MMA warp 7, drain warps 8-15 (64 columns each)
+constexpr int kP2CopyWarps = 27;
+constexpr int kP2Producers = 32 * kP2CopyWarps;  // threads of the copy warps 0-26
+constexpr int kP2Threads = 1024;                 // copy warps 0-26, MMA warp 27, drain warps 28-31
 constexpr int kP2BarBytes = 8 * (2 * kP2Stages + 2 * kP2Bufs + 1);
 constexpr size_t kP2Smem = (size_t)kP2Stages * kTcStage + kP2BarBytes + 16;
 
@@ -427,14 +428,14 @@ __global__ void __launch_bounds__(kP2Threads, 1)
     }
     for (int i = 0; i < kP2Bufs; ++i) {
       mbar_init(ready + 8u * i, 1);
-      mbar_init(freeb + 8u * i, 256);
+      mbar_init(freeb + 8u * i, 128);
     }
     mbar_init(done, 1);
     *abort_flag = 0;
     mbar_init_fence();
   }
   if (warp == 0) {
-    tmem_alloc(smem_u32(slot), 128 * kP2Bufs);
+    tmem_alloc(smem_u32(slot), 512);
     tmem_relinquish();
   }
   tc_fence_before();
@@ -448,7 +449,7 @@ __global__ void __launch_bounds__(kP2Threads, 1)
     *abort_flag = 1;
   };
 
-  if (warp < 7) {  // ---- producers
+  if (warp < kP2CopyWarps) {  // ---- producers
     const int pt = tid;
     long long j = 0, arrived = 0;  // steps issued; steps announced
     for (int b = blockIdx.x; b < nblocks && !failed; b += stride) {
@@ -514,7 +515,7 @@ __global__ void __launch_bounds__(kP2Threads, 1)
     if (pt == 0)
       for (long long jj = j > kP2Stages ? j - kP2Stages : 0; jj < j; ++jj)
         mbar_wait(full + 8u * (uint32_t)(jj % kP2Stages), (uint32_t)((jj / kP2Stages) & 1), 1000000000ull);
-  } else if (warp == 7) {  // ---- MMA issuer
+  } else if (warp == kP2CopyWarps) {  // ---- MMA issuer
     if (lane == 0) {
       const uint64_t desc0 = tc_sdesc(sbase, 2048, 128);  // A, T blocks and X's image: SBO 128, LBO 2048
       long long j = 0;
@@ -579,16 +580,25 @@ __global__ void __launch_bounds__(kP2Threads, 1)
       }
       tc_commit(done);  // arrives once every MMA issued above is done
     }
-  } else {  // ---- drain warps 8-15: TMEM lanes 32 (warp % 4) .. (row m of the block), columns 64 hf ..
-    const int m = (warp & 3) * 32 + lane, hf = (warp - 8) >> 2;
+  } else {  // ---- drain warps 28-31: TMEM lanes 32 (warp % 4) .., row m of the block
+    // Each chain is added to the block's running sums kept in tensor memory
+    // (columns 256-383: read, FP32 round-to-nearest add, write back); the last
+    // chain's sums go to Y.  Few registers per thread (at most 64 in a CTA of
+    // 32 warps), so that 27 warps can copy.
+    const int m = (warp & 3) * 32 + lane;
     const uint32_t my_lanes = (uint32_t)((warp & 3) * 32) << 16;
-    float acc[64];
-#pragma unroll
-    for (int i = 0; i < 64; ++i) acc[i] = 0.f;
+    const uint32_t tsum = tmem + my_lanes + 256u;
     int chain = -1;
     for (int b = blockIdx.x; b < nblocks && !failed; b += stride) {
       const int nsteps = step_ptr[b + 1] - step_ptr[b];
       const int nchains = (nsteps + kP2Chain - 1) / kP2Chain;
+      const int G = tile0 + 4 * b + (m >> 5);
+      int row = -1;
+      if (G < tile_end) {
+        const int x = tile_leaf[G];
+        const int r = leaf_off[x] + 32 * (G - leaf_tile0[x]) + (m & 31);
+        if (r < leaf_off[x + 1]) row = r;
+      }
       for (int c = 0; c < nchains; ++c) {
         ++chain;
         const uint32_t bb = (uint32_t)(chain % kP2Bufs);
@@ -597,30 +607,34 @@ __global__ void __launch_bounds__(kP2Threads, 1)
           break;
         }
         tc_fence_after();
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        const bool first = c == 0, last = c + 1 == nchains;
+        float* yq = Y + (row >= 0 ? row : 0);
+#pragma unroll 1
+        for (int q = 0; q < 8; ++q, yq += (size_t)16 * ldy) {
           uint32_t v[16];
-          tc_ld16(tmem + my_lanes + bb * 128u + (uint32_t)(hf * 64 + q * 16), v);
-          tc_wait_ld();
+          tc_ld16(tmem + my_lanes + bb * 128u + (uint32_t)(q * 16), v);
+          if (!first) {
+            uint32_t sm[16];
+            tc_ld16(tsum + (uint32_t)(q * 16), sm);
+            tc_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 16; ++i) acc[q * 16 + i] += __uint_as_float(v[i]);
+            for (int e = 0; e < 16; ++e) v[e] = __float_as_uint(__uint_as_float(v[e]) + __uint_as_float(sm[e]));
+          } else {
+            tc_wait_ld();
+          }
+          if (!last) {
+            tc_st16(tsum + (uint32_t)(q * 16), v);
+          } else if (row >= 0) {
+            float* y = yq;
+#pragma unroll
+            for (int e = 0; e < 16; ++e, y += ldy)
+              if (q * 16 + e < nr) *y = __uint_as_float(v[e]);
+          }
         }
+        if (!last) tc_wait_st();
         tc_fence_before();
         mbar_arrive(freeb + 8u * bb);
       }
-      if (failed) break;
-      const int G = tile0 + 4 * b + (m >> 5);
-      if (G < tile_end) {
-        const int x = tile_leaf[G];
-        const int row = leaf_off[x] + 32 * (G - leaf_tile0[x]) + (m & 31);
-        if (row < leaf_off[x + 1]) {
-#pragma unroll
-          for (int c = 0; c < 64; ++c)
-            if (64 * hf + c < nr) Y[(size_t)(64 * hf + c) * ldy + row] = acc[c];
-        }
-      }
-#pragma unroll
-      for (int i = 0; i < 64; ++i) acc[i] = 0.f;
     }
   }
   if (failed) atomicExch(err, 1);
@@ -629,7 +643,7 @@ __global__ void __launch_bounds__(kP2Threads, 1)
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    tmem_dealloc(tmem, 128 * kP2Bufs);
+    tmem_dealloc(tmem, 512);
   }
 }
 
