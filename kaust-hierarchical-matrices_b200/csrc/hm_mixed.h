@@ -133,7 +133,7 @@ struct MxPlan {
   std::vector<MxDense> h_dense;           // host copy
   std::vector<MxLoc> h_locs;              // every factor and dense block converted into the panels
   std::vector<std::pair<const float*, int>> loc_index;  // h_locs by key, sorted (built on first use)
-  int chunk_tiles = 128, group_tiles = 4;  // phase-1 unit shape (schedule parameters)
+  int chunk_tiles = 128, group_tiles = 8;  // phase-1 unit shape (schedule parameters; measured best at 16 RHS)
   bool p1_ring = false;                    // phase 1 by persistent warps with a cp.async ring
   int num_sms = 148;
   // 128-column passes (BF16 format) on tcgen05 (hm_mixed_tc.cu): phase-1
