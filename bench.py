@@ -334,14 +334,19 @@ TRAFFIC_SOURCES = ["csrc/hm_mixed.cu", "csrc/hm_mixed.h", "csrc/hm_fp32.cu", "cs
 
 
 def kernel_source_digest():
-    """SHA-256 over the product kernels' sources: a DRAM-traffic capture is
-    used only while the kernels it measured are unchanged."""
+    """SHA-256 over the product kernels' sources, code only (// comments and
+    blank lines removed): a DRAM-traffic capture is used only while the
+    kernels it measured are unchanged."""
     import hashlib
+    import re
 
     h = hashlib.sha256()
     for f in TRAFFIC_SOURCES:
-        with open(os.path.join(PKG, f), "rb") as fh:
-            h.update(fh.read())
+        with open(os.path.join(PKG, f), encoding="utf-8") as fh:
+            for line in fh:
+                code = re.sub(r"//.*$", "", line).strip()
+                if code:
+                    h.update(code.encode() + b"\n")
     return h.hexdigest()
 
 

@@ -9,6 +9,9 @@
 //   k_mx_reduce   (panels of several row chunks only) the partials summed in
 //                 chunk order, stored as T
 //   k_mx_p2       Y = sum over the ancestors' panels of U T, plus dense blocks
+// (Passes of 65-128 right-hand sides run on the tcgen05 kernels of
+// hm_mixed_tc.cu unless the schedule says wide_tc=0; k_mx_split_x then writes
+// X's image for them instead of the fragments.)
 // "Stored as T": the projection on a factor column is the coefficient of the
 // mirror block's factor column (block (s,t) = U V^T: V^T X_t multiplies U,
 // U^T X_s multiplies V), so each column of P is written, split into BF16

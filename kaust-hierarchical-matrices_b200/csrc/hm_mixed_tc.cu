@@ -32,9 +32,10 @@
 // below the BF16 hi + lo rounding of T.  At a unit's end each drain thread
 // stores its column (its TMEM lane): as T (into the mirror column's slots,
 // split hi + lo or hi only) when the panel is projected in one row chunk,
-// else as the chunk's partial S (per column its 128 FP32 sums, contiguous).  Every wait is bounded; a wait that gives up
-// raises an abort flag that the other roles see, sets the error word, and
-// the kernel ends after every issued copy and MMA has completed.
+// else as the chunk's partial S (per column its 128 FP32 sums, contiguous).
+// Every wait is bounded; a wait that gives up raises an abort flag that the
+// other roles see, sets the error word, and the kernel ends after every
+// issued copy and MMA has completed.
 //
 // T of such a pass is kept in 2 KB blocks, one per 8 columns and part (hi,
 // lo): the MN-major core-matrix image of B = T for phase 2 (right-hand sides
@@ -50,8 +51,8 @@
 // the block's tiles that a source does not cover are zero.  Dense blocks take
 // their columns in X's row order rho so that B is X's image of the column
 // cluster's tile.  Panels' columns with low parts take three products per 16
-// columns; the others one per 16 columns, 32 columns per step; dense blocks
-// three per 16 columns, 32 per step.
+// columns, 32 columns per step; the others one per 16 columns, 64 per step;
+// dense blocks three per 16 columns, 32 per step.
 #include "hm_hmatrix.h"
 #include "hm_mixed.h"
 #include "hm_mma.cuh"
