@@ -653,11 +653,14 @@ __global__ void __launch_bounds__(kP2Threads, 1)
 hm_status mixed_tc_pass(hm_hmatrix_s* h, int nr, const uint4* Xtc, float* S, uint4* Tb, float* Y, int ldy,
                         cudaStream_t s, KernelMarks* km) {
   MxPlan& M = h->mx;
-  static bool attr = false;
-  if (!attr) {
+  // the kernels' shared-memory limit, once per device of this process
+  static unsigned long long attr_done = 0;
+  int dev = 0;
+  HM_CUDA(cudaGetDevice(&dev));
+  if (dev >= 64 || !((attr_done >> dev) & 1ull)) {
     HM_CUDA(cudaFuncSetAttribute(k_mx_p1_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP1Smem));
     HM_CUDA(cudaFuncSetAttribute(k_mx_p2_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2Smem));
-    attr = true;
+    if (dev < 64) attr_done |= 1ull << dev;
   }
   const long long xbytes = 4ll * h->n * 128;  // X's image: hi + lo of 128 right-hand sides
   if (M.num_tc_units > 0) {
