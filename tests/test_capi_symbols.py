@@ -126,6 +126,23 @@ def test_solver_and_file_entry_points_validate_without_gpu(tmp_path):
     assert lib.hm_hmatrix_load(None, None, b"x", None, None) == 1
 
 
+def test_check_and_schedule_entry_points_validate_without_gpu():
+    """hm_hmatrix_check (the report of a device-side wait that gave up) and
+    hm_schedule_set refuse null arguments before any CUDA call."""
+    path = os.path.join(PKG, "libhmb200.so")
+    if not os.path.exists(path):
+        pytest.skip("libhmb200.so not built")
+    lib = ctypes.CDLL(path)
+    lib.hm_last_error.restype = ctypes.c_char_p
+    P = ctypes.c_void_p
+    lib.hm_hmatrix_check.argtypes = [P, P]
+    lib.hm_schedule_set.argtypes = [P, ctypes.c_char_p, P]
+    assert lib.hm_hmatrix_check(None, None) == 1
+    assert b"null matrix" in lib.hm_last_error()
+    assert lib.hm_schedule_set(None, b"mixed chunk_tiles=128 group_tiles=8 p1_ring=0 wide_tc=1 tc_chunk=32", None) == 1
+    assert lib.hm_schedule_set(None, None, None) == 1
+
+
 def test_python_wrappers_check_vector_shapes():
     """The C ABI trusts the sizes it is given; the Python wrappers check a
     block of vectors (float32 CUDA tensor, shape (n, nrhs)) before calling it."""
